@@ -208,8 +208,10 @@ def _run_ref(args, threads=0):
     env = dict(os.environ)
     if threads:
         env["PARLAY_NUM_THREADS"] = str(threads)
-    r = subprocess.run([REF_HARNESS] + [str(a) for a in args], capture_output=True, env=env,
-                       check=True)
+    # knn_index::batch_insert opens ./parlay_graph_log (include/index.h:224): run elsewhere
+    with tempfile.TemporaryDirectory() as cwd:
+        r = subprocess.run([REF_HARNESS] + [str(a) for a in args], capture_output=True, env=env,
+                           check=True, cwd=cwd)
     return r.stdout.decode("utf-8", "replace")
 
 
