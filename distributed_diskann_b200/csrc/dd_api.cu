@@ -1,0 +1,740 @@
+// Host side of the C ABI (include/dd_gpu.h): handle management, the batched
+// build driver (round schedule of src/bsp_index.hpp:141-246 collapsed onto one
+// device-resident index) and the search / ground-truth entry points.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "../../include/dd_gpu.h"
+#include "dd_common.cuh"
+#include "kernels.cuh"
+#include "sort_emul.cuh"
+
+using namespace ddk;
+
+struct dd_index {
+  int dtype = 0, metric = 0;
+  uint64_t n = 0;
+  uint32_t d = 0, R = 0, Rp = 0;
+  uint64_t stride = 0;  // device row stride in bytes
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = 0;
+  uint8_t* points = nullptr;
+  uint32_t* graph = nullptr;
+  uint32_t* err = nullptr;
+  std::string last_error;
+  uint64_t launches = 0;
+  // build scratch (grown on demand, kept for reuse)
+  uint64_t bcap = 0;        // batch capacity of the scratch below
+  uint32_t* new_out = nullptr;
+  uint32_t* stat_vis = nullptr;
+  uint32_t* stat_cmps = nullptr;
+  uint32_t* keys = nullptr;
+  uint32_t* cnt = nullptr;
+  uint32_t* cursor = nullptr;
+  uint32_t* touched = nullptr;
+  uint32_t* seg_start = nullptr;
+  uint32_t* counters = nullptr;
+  uint32_t* big = nullptr;
+  uint32_t* block_sums = nullptr;
+  unsigned long long* acc = nullptr;  // [0] visited [1] cmps [2] groups [3] prunes [4] cands [5] big
+  uint32_t* gcand = nullptr;
+  float* gkey = nullptr;
+  int* gleaf = nullptr;
+  uint64_t gcap = 0;
+};
+
+namespace {
+
+constexpr uint32_t kBigSlots = 16;
+constexpr int kSearchWarpsPerCta = 2;
+
+int fail(dd_index* h, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (h) h->last_error = buf;
+  return code;
+}
+
+#define CK(call)                                                                    \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess)                                                          \
+      return fail(h, e_ == cudaErrorMemoryAllocation ? DD_ERR_OOM : DD_ERR_CUDA,    \
+                  "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+uint32_t esize(int dtype) { return dtype == DD_F32 ? 4u : 1u; }
+
+IndexView view(dd_index* h) {
+  IndexView v;
+  v.dtype = h->dtype;
+  v.metric = h->metric;
+  v.points = h->points;
+  v.stride = h->stride;
+  v.graph = h->graph;
+  v.Rp = h->Rp;
+  v.R = h->R;
+  v.n = h->n;
+  v.d = h->d;
+  v.err = h->err;
+  return v;
+}
+
+template <typename T>
+cudaError_t dalloc(T** p, uint64_t count) {
+  return cudaMalloc((void**)p, std::max<uint64_t>(count, 1) * sizeof(T));
+}
+
+void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+
+int check_error_word(dd_index* h) {
+  uint32_t e = 0;
+  CK(cudaMemcpyAsync(&e, h->err, 4, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (e) {
+    cudaMemsetAsync(h->err, 0, 4, h->stream);
+    std::string m = "device error:";
+    if (e & DD_EBAD_ID) m += " neighbour id out of range;";
+    if (e & DD_EVIS_CAP) m += " visited list exceeded its capacity (raise vcap);";
+    if (e & DD_ECAND_CAP) m += " a per-query beam width was 0, below k or above Lmax;";
+    if (e & DD_EDEGREE) m += " row degree exceeds R;";
+    if (e & DD_ESEG_CAP) m += " reverse-edge group exceeded the workspace;";
+    return fail(h, DD_ERR_DEVICE, "%s", m.c_str());
+  }
+  return DD_OK;
+}
+
+// (floor, ceiling) rounds: src/bsp_index.hpp:162-166, 238-246 (identity order)
+std::vector<std::pair<uint64_t, uint64_t>> schedule(uint64_t n, uint64_t max_build, double frac,
+                                                    int knn_mode) {
+  uint64_t m = n;
+  if (knn_mode) frac = 1.0;
+  else if (max_build != 0) m = std::min<uint64_t>(max_build, m);
+  size_t mb = std::min((size_t)(frac * (float)m), (size_t)1000000ul);
+  if (mb == 0) mb = m;
+  std::vector<std::pair<uint64_t, uint64_t>> r;
+  size_t inc = 0, count = 0;
+  while (count < m) {
+    size_t fl, ce;
+    if (std::pow(2.0, (double)inc) <= (double)mb) {
+      fl = (size_t)std::pow(2.0, (double)inc) - 1;
+      ce = std::min((size_t)std::pow(2.0, (double)(inc + 1)), (size_t)m) - 1;
+      count = ce;
+    } else {
+      fl = count;
+      ce = std::min(count + mb, (size_t)m);
+      count += mb;
+    }
+    r.push_back({fl, ce});
+    inc++;
+  }
+  return r;
+}
+
+int ensure_build_scratch(dd_index* h, uint64_t B) {
+  if (!h->cnt) {
+    CK(dalloc(&h->cnt, h->n));
+    CK(dalloc(&h->cursor, h->n));
+    CK(cudaMemsetAsync(h->cnt, 0, h->n * 4, h->stream));
+    CK(dalloc(&h->counters, 8));
+    CK(dalloc(&h->block_sums, kScanBlocks + 1));
+    CK(dalloc(&h->acc, 8));
+  }
+  if (B <= h->bcap) return DD_OK;
+  dfree(h->new_out); dfree(h->stat_vis); dfree(h->stat_cmps); dfree(h->keys);
+  dfree(h->touched); dfree(h->seg_start); dfree(h->big);
+  dfree(h->gcand); dfree(h->gkey); dfree(h->gleaf);
+  uint64_t E = B * h->Rp;
+  uint64_t T = std::min<uint64_t>(h->n, E);
+  CK(dalloc(&h->new_out, E));
+  CK(dalloc(&h->stat_vis, B));
+  CK(dalloc(&h->stat_cmps, B));
+  CK(dalloc(&h->keys, E));
+  CK(dalloc(&h->touched, T));
+  CK(dalloc(&h->seg_start, T));
+  CK(dalloc(&h->big, T));
+  h->gcap = B + h->Rp;
+  CK(dalloc(&h->gcand, kBigSlots * h->gcap));
+  CK(dalloc(&h->gkey, kBigSlots * h->gcap));
+  CK(dalloc(&h->gleaf, kBigSlots * (2 * h->gcap + ddsort::stack_ints((int)h->gcap))));
+  h->bcap = B;
+  return DD_OK;
+}
+
+// the reverse-edge scratch of a handle
+ReverseScratch make_rs(dd_index* h) {
+  ReverseScratch rs;
+  rs.cnt = h->cnt;
+  rs.cursor = h->cursor;
+  rs.touched = h->touched;
+  rs.seg_start = h->seg_start;
+  rs.keys = h->keys;
+  rs.counters = h->counters;
+  rs.big = h->big;
+  rs.block_sums = h->block_sums;
+  rs.gcand = h->gcand;
+  rs.gkey = h->gkey;
+  rs.gleaf = h->gleaf;
+  rs.gcap = h->gcap;
+  return rs;
+}
+
+__global__ void k_accumulate(const uint32_t* stat_vis, const uint32_t* stat_cmps, uint32_t B,
+                             const uint32_t* counters, unsigned long long* acc) {
+  unsigned long long sv = 0, sc = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < B; i += gridDim.x * blockDim.x) {
+    sv += stat_vis[i];
+    sc += stat_cmps[i];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sv += __shfl_down_sync(0xffffffffu, sv, o);
+    sc += __shfl_down_sync(0xffffffffu, sc, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&acc[0], sv);
+    atomicAdd(&acc[1], sc);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    atomicAdd(&acc[2], (unsigned long long)counters[0]);
+    atomicAdd(&acc[3], (unsigned long long)counters[2]);
+    atomicAdd(&acc[4], (unsigned long long)counters[3]);
+    atomicAdd(&acc[5], (unsigned long long)counters[1]);
+  }
+}
+
+int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& rounds, double alpha,
+                const dd_build_params* P, const WarpLayout& lay, int grid_max, cudaEvent_t* ev,
+                float* t_search, float* t_rev) {
+  IndexView ix = view(h);
+  for (auto& rd : rounds) {
+    uint64_t B = rd.second > rd.first ? rd.second - rd.first : 0;
+    if (!B) continue;
+    RoundArgs ra;
+    ra.floor = rd.first;
+    ra.B = (uint32_t)B;
+    ra.L = P->L;
+    ra.alpha = alpha;
+    ra.start = P->start_point;
+    ra.new_out = h->new_out;
+    ra.stat_vis = h->stat_vis;
+    ra.stat_cmps = h->stat_cmps;
+    CK(cudaMemsetAsync(h->counters, 0, 8 * 4, h->stream));
+    if (ev) CK(cudaEventRecord(ev[0], h->stream));
+    int grid = (int)std::min<uint64_t>((B + kSearchWarpsPerCta - 1) / kSearchWarpsPerCta,
+                                       (uint64_t)grid_max);
+    launch_search_prune(ix, ra, lay, kSearchWarpsPerCta, grid, h->stream);
+    launch_apply_rows(ix, ra, h->stream);
+    if (ev) CK(cudaEventRecord(ev[1], h->stream));
+    launch_reverse(ix, ra, make_rs(h), h->stream, h->sm_count);
+    launch_reverse_big(ix, ra, make_rs(h), kBigSlots, h->stream);
+    h->launches += 9;
+    if (P->collect_stats) {
+      k_accumulate<<<64, 256, 0, h->stream>>>(h->stat_vis, h->stat_cmps, (uint32_t)B, h->counters,
+                                              h->acc);
+      h->launches++;
+    }
+    if (ev) {
+      CK(cudaEventRecord(ev[2], h->stream));
+      CK(cudaEventSynchronize(ev[2]));
+      float a = 0, b = 0;
+      cudaEventElapsedTime(&a, ev[0], ev[1]);
+      cudaEventElapsedTime(&b, ev[1], ev[2]);
+      *t_search += a;
+      *t_rev += b;
+    }
+    CK(cudaGetLastError());
+  }
+  return DD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dd_create(int dtype, int metric, uint64_t n, uint32_t d, uint32_t R, int device,
+              dd_index** out) {
+  dd_index* h = nullptr;
+  if (!out) return DD_ERR_ARG;
+  *out = nullptr;
+  if (dtype < 0 || dtype > 2 || metric < 0 || metric > 1) return DD_ERR_ARG;
+  if (n == 0 || n >= 0x7fffffffull || d == 0 || R == 0) return DD_ERR_ARG;
+  if (R > kMaxRp) return DD_ERR_UNSUPPORTED;
+  if ((uint64_t)d * esize(dtype) > 1024) return DD_ERR_UNSUPPORTED;
+  h = new dd_index();
+  h->dtype = dtype;
+  h->metric = metric;
+  h->n = n;
+  h->d = d;
+  h->R = R;
+  h->Rp = (R + 3) & ~3u;
+  h->stride = ((uint64_t)d * esize(dtype) + 63) & ~(uint64_t)63;
+  h->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&h->points, n * h->stride);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&h->graph, n * h->Rp * 4ull);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&h->err, 16);
+  if (e == cudaSuccess) e = cudaMemset(h->points, 0, n * h->stride);
+  if (e == cudaSuccess) e = cudaMemset(h->graph, 0xff, n * h->Rp * 4ull);
+  if (e == cudaSuccess) e = cudaMemset(h->err, 0, 16);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    int code = e == cudaErrorMemoryAllocation ? DD_ERR_OOM : DD_ERR_CUDA;
+    dd_destroy(h);
+    return code;
+  }
+  *out = h;
+  return DD_OK;
+}
+
+int dd_destroy(dd_index* h) {
+  if (!h) return DD_OK;
+  cudaSetDevice(h->device);
+  void* ptrs[] = {h->points, h->graph, h->err, h->new_out, h->stat_vis, h->stat_cmps, h->keys,
+                  h->cnt, h->cursor, h->touched, h->seg_start, h->counters, h->big,
+                  h->block_sums, h->acc, h->gcand, h->gkey, h->gleaf};
+  for (void* p : ptrs) dfree(p);
+  delete h;
+  return DD_OK;
+}
+
+const char* dd_last_error(const dd_index* h) { return h ? h->last_error.c_str() : "null handle"; }
+
+int dd_set_stream(dd_index* h, void* stream) {
+  if (!h) return DD_ERR_ARG;
+  h->stream = (cudaStream_t)stream;
+  return DD_OK;
+}
+
+int dd_upload_points(dd_index* h, const void* rows, uint64_t row_stride_bytes) {
+  if (!h || !rows) return DD_ERR_ARG;
+  uint64_t rb = (uint64_t)h->d * esize(h->dtype);
+  if (row_stride_bytes < rb) return fail(h, DD_ERR_ARG, "row stride %llu < row bytes %llu",
+                                         (unsigned long long)row_stride_bytes, (unsigned long long)rb);
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpy2DAsync(h->points, h->stride, rows, row_stride_bytes, rb, h->n,
+                       cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DD_OK;
+}
+
+int dd_upload_points_device(dd_index* h, const void* rows, uint64_t row_stride_bytes) {
+  if (!h || !rows) return DD_ERR_ARG;
+  uint64_t rb = (uint64_t)h->d * esize(h->dtype);
+  if (row_stride_bytes < rb) return fail(h, DD_ERR_ARG, "row stride too small");
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpy2DAsync(h->points, h->stride, rows, row_stride_bytes, rb, h->n,
+                       cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DD_OK;
+}
+
+int dd_load_points_file(dd_index* h, const char* path) {
+  if (!h || !path) return DD_ERR_ARG;
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return fail(h, DD_ERR_IO, "cannot open %s", path);
+  uint32_t hdr[2];
+  f.read((char*)hdr, 8);
+  if (!f || hdr[0] != h->n || hdr[1] != h->d)
+    return fail(h, DD_ERR_IO, "%s: header [%u, %u] does not match the index", path, hdr[0], hdr[1]);
+  uint64_t rb = (uint64_t)h->d * esize(h->dtype);
+  std::vector<char> buf(rb * h->n);
+  f.read(buf.data(), (std::streamsize)buf.size());
+  if (!f) return fail(h, DD_ERR_IO, "%s: truncated", path);
+  return dd_upload_points(h, buf.data(), rb);
+}
+
+int dd_upload_graph(dd_index* h, const uint32_t* rows) {
+  if (!h || !rows) return DD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  uint32_t* tmp = nullptr;
+  CK(dalloc(&tmp, h->n * (h->R + 1)));
+  cudaError_t e = cudaMemcpyAsync(tmp, rows, h->n * (h->R + 1) * 4ull, cudaMemcpyHostToDevice,
+                                  h->stream);
+  if (e == cudaSuccess) {
+    launch_from_ref_rows(view(h), tmp, h->stream);
+    e = cudaStreamSynchronize(h->stream);
+  }
+  cudaFree(tmp);
+  CK(e);
+  return check_error_word(h);
+}
+
+int dd_download_graph(dd_index* h, uint32_t* rows) {
+  if (!h || !rows) return DD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  uint32_t* tmp = nullptr;
+  CK(dalloc(&tmp, h->n * (h->R + 1)));
+  launch_to_ref_rows(view(h), tmp, h->stream);
+  cudaError_t e = cudaMemcpyAsync(rows, tmp, h->n * (h->R + 1) * 4ull, cudaMemcpyDeviceToHost,
+                                  h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(tmp);
+  CK(e);
+  return DD_OK;
+}
+
+int dd_save_graph_file(dd_index* h, const char* path) {
+  if (!h || !path) return DD_ERR_ARG;
+  std::vector<uint32_t> g(h->n * (h->R + 1));
+  int rc = dd_download_graph(h, g.data());
+  if (rc) return rc;
+  // include/utils/graph.h:178-200: [n][R][degrees][edges of each row]
+  std::ofstream f(path, std::ios::binary);
+  if (!f) return fail(h, DD_ERR_IO, "cannot open %s", path);
+  uint32_t pre[2] = {(uint32_t)h->n, h->R};
+  f.write((const char*)pre, 8);
+  for (uint64_t i = 0; i < h->n; i++) f.write((const char*)&g[i * (h->R + 1)], 4);
+  for (uint64_t i = 0; i < h->n; i++)
+    f.write((const char*)&g[i * (h->R + 1) + 1], 4ull * g[i * (h->R + 1)]);
+  if (!f) return fail(h, DD_ERR_IO, "write failed: %s", path);
+  return DD_OK;
+}
+
+int dd_load_graph_file(dd_index* h, const char* path) {
+  if (!h || !path) return DD_ERR_ARG;
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return fail(h, DD_ERR_IO, "cannot open %s", path);
+  uint32_t pre[2];
+  f.read((char*)pre, 8);
+  if (!f || pre[0] != h->n || pre[1] != h->R)
+    return fail(h, DD_ERR_IO, "%s: [n, R] = [%u, %u] does not match the index", path, pre[0], pre[1]);
+  std::vector<uint32_t> deg(h->n);
+  f.read((char*)deg.data(), 4ll * h->n);
+  std::vector<uint32_t> g(h->n * (h->R + 1), 0);
+  for (uint64_t i = 0; i < h->n; i++) {
+    if (deg[i] > h->R) return fail(h, DD_ERR_IO, "%s: row %llu degree %u > R", path,
+                                   (unsigned long long)i, deg[i]);
+    g[i * (h->R + 1)] = deg[i];
+    f.read((char*)&g[i * (h->R + 1) + 1], 4ll * deg[i]);
+  }
+  if (!f) return fail(h, DD_ERR_IO, "%s: truncated", path);
+  return dd_upload_graph(h, g.data());
+}
+
+int dd_schedule(uint64_t n, uint64_t max_build, double max_fraction, int knn_mode,
+                uint64_t* floors, uint64_t* ceilings, uint64_t cap, uint64_t* nrounds) {
+  auto r = schedule(n, max_build, max_fraction, knn_mode);
+  for (size_t i = 0; i < r.size() && i < cap; i++) {
+    floors[i] = r[i].first;
+    ceilings[i] = r[i].second;
+  }
+  if (nrounds) *nrounds = r.size();
+  return DD_OK;
+}
+
+int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
+  if (!h || !P) return DD_ERR_ARG;
+  if (P->L == 0 || P->L > kMaxL) return fail(h, DD_ERR_UNSUPPORTED, "L must be in [1, %u]", kMaxL);
+  uint32_t start = P->knn_mode ? 0 : P->start_point;  // include/index.h:127
+  if (start >= h->n) return fail(h, DD_ERR_ARG, "start point %u >= n", start);
+  if (!(P->alpha > 0)) return fail(h, DD_ERR_ARG, "alpha must be positive");
+  CK(cudaSetDevice(h->device));
+  h->launches = 0;
+  auto rounds = schedule(h->n, P->max_build, P->max_fraction, P->knn_mode);
+  uint64_t Bmax = 1;
+  for (auto& r : rounds) Bmax = std::max<uint64_t>(Bmax, r.second > r.first ? r.second - r.first : 0);
+  int rc = ensure_build_scratch(h, Bmax);
+  if (rc) return rc;
+  uint32_t vcap = P->vcap ? P->vcap : 4 * P->L;
+  WarpLayout lay = make_search_layout(h->d, h->dtype, P->L, h->Rp, vcap, true);
+  if ((size_t)lay.total * kSearchWarpsPerCta > 227 * 1024)
+    return fail(h, DD_ERR_UNSUPPORTED, "per-warp shared memory %u B too large (L=%u)", lay.total, P->L);
+  int bps = 1;
+  {
+    size_t sm = (size_t)lay.total * kSearchWarpsPerCta;
+    bps = std::max(1, (int)((228 * 1024) / (sm + 1024)));
+  }
+  int grid_max = bps * h->sm_count;
+
+  // empty graph (the reference starts from Graph(R, n): all degrees 0)
+  CK(cudaMemsetAsync(h->graph, 0xff, h->n * h->Rp * 4ull, h->stream));
+  CK(cudaMemsetAsync(h->acc, 0, 8 * 8, h->stream));
+  CK(cudaMemsetAsync(h->err, 0, 4, h->stream));
+  cudaEvent_t e0, e1, ev[3];
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  bool timed = stats != nullptr;
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  CK(cudaEventRecord(e0, h->stream));
+  float ts = 0, tr = 0;
+  // RoundArgs fields that depend on the pass are set inside pass_rounds
+  dd_build_params Q = *P;
+  Q.start_point = start;
+  if (P->two_pass) {
+    rc = pass_rounds(h, rounds, 1.0, &Q, lay, grid_max, timed ? ev : nullptr, &ts, &tr);
+    if (rc) return rc;
+  }
+  rc = pass_rounds(h, rounds, P->alpha, &Q, lay, grid_max, timed ? ev : nullptr, &ts, &tr);
+  if (rc) return rc;
+  if (P->knn_mode) {
+    launch_sort_rows(view(h), h->stream);
+    h->launches++;
+  }
+  CK(cudaEventRecord(e1, h->stream));
+  CK(cudaEventSynchronize(e1));
+  CK(cudaGetLastError());
+  rc = check_error_word(h);
+  if (stats) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    unsigned long long acc[8] = {0};
+    cudaMemcpy(acc, h->acc, sizeof acc, cudaMemcpyDeviceToHost);
+    std::memset(stats, 0, sizeof *stats);
+    stats->rounds = rounds.size() * (P->two_pass ? 2 : 1);
+    stats->visited = acc[0];
+    stats->dist_cmps = acc[1];
+    stats->groups = acc[2];
+    stats->reverse_prunes = acc[3];
+    stats->prune_cands = acc[4];
+    stats->big_groups = acc[5];
+    stats->build_ms = ms;
+    stats->search_prune_ms = ts;
+    stats->reverse_ms = tr;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (auto& e : ev) cudaEventDestroy(e);
+  return rc;
+}
+
+int dd_search_device(dd_index* h, const void* queries, uint64_t nq, uint64_t qstride,
+                     const uint32_t* L_per_query, uint32_t Lmax, uint32_t k, double cut,
+                     uint64_t limit, uint32_t degree_limit, uint32_t start, int skip_self,
+                     uint32_t* ids, float* dists, uint32_t* visited, uint32_t* cmps) {
+  if (!h || !queries || !L_per_query || !ids || !dists) return DD_ERR_ARG;
+  if (nq == 0) return DD_OK;
+  if (Lmax == 0 || Lmax > kMaxL) return fail(h, DD_ERR_UNSUPPORTED, "L must be in [1, %u]", kMaxL);
+  if (k == 0 || k > Lmax) return fail(h, DD_ERR_ARG, "k must be in [1, L]");  // beamSearch.h:327-331
+  if (start >= h->n) return fail(h, DD_ERR_ARG, "start point >= n");
+  if (qstride % 16) return fail(h, DD_ERR_ARG, "device query stride must be a multiple of 16");
+  CK(cudaSetDevice(h->device));
+  h->launches = 0;
+  WarpLayout lay = make_search_layout(h->d, h->dtype, Lmax, h->Rp, 2 * Lmax + 64, false);
+  int wpc = 4;
+  while (wpc > 1 && (size_t)lay.total * wpc > 227 * 1024) wpc >>= 1;
+  if ((size_t)lay.total * wpc > 227 * 1024)
+    return fail(h, DD_ERR_UNSUPPORTED, "query shared memory %u B too large", lay.total);
+  size_t sm = (size_t)lay.total * wpc;
+  int bps = std::max(1, (int)((228 * 1024) / (sm + 1024)));
+  int grid = (int)std::min<uint64_t>((nq + wpc - 1) / wpc, (uint64_t)bps * h->sm_count);
+  QueryArgs qa;
+  qa.queries = (const uint8_t*)queries;
+  qa.qstride = qstride;
+  qa.nq = nq;
+  qa.Ls = L_per_query;
+  qa.Lmax = Lmax;
+  qa.k = k;
+  qa.cut = cut;
+  qa.limit = limit ? limit : h->n;
+  qa.degree_limit = degree_limit ? std::min(degree_limit, h->R) : h->R;
+  qa.start = start;
+  qa.skip_self = skip_self;
+  qa.ids = ids;
+  qa.dists = dists;
+  qa.visited = visited;
+  qa.cmps = cmps;
+  launch_query(view(h), qa, lay, wpc, grid, h->stream);
+  h->launches = 1;
+  CK(cudaGetLastError());
+  return DD_OK;
+}
+
+int dd_search(dd_index* h, const void* queries, uint64_t nq, uint64_t qstride,
+              const uint32_t* L_per_query, uint32_t k, double cut, uint64_t limit,
+              uint32_t degree_limit, uint32_t start, int skip_self, uint32_t* ids, float* dists,
+              uint32_t* visited, uint32_t* cmps) {
+  if (!h || !queries || !L_per_query || !ids || !dists) return DD_ERR_ARG;
+  if (nq == 0) return DD_OK;
+  CK(cudaSetDevice(h->device));
+  uint64_t rb = (uint64_t)h->d * esize(h->dtype);
+  uint64_t ds = h->stride;
+  uint32_t Lmax = 0;
+  for (uint64_t i = 0; i < nq; i++) Lmax = std::max(Lmax, L_per_query[i]);
+  uint8_t* dq = nullptr;
+  uint32_t *dL = nullptr, *di = nullptr, *dv = nullptr, *dc = nullptr;
+  float* dd = nullptr;
+  CK(dalloc(&dq, nq * ds));
+  int rc = DD_OK;
+  cudaError_t e = dalloc(&dL, nq);
+  if (e == cudaSuccess) e = dalloc(&di, nq * k);
+  if (e == cudaSuccess) e = dalloc(&dd, nq * k);
+  if (e == cudaSuccess) e = dalloc(&dv, nq);
+  if (e == cudaSuccess) e = dalloc(&dc, nq);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dq, 0, nq * ds, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(dq, ds, queries, qstride, rb, nq, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dL, L_per_query, nq * 4, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) {
+    rc = dd_search_device(h, dq, nq, ds, dL, Lmax, k, cut, limit, degree_limit, start, skip_self,
+                          di, dd, dv, dc);
+    if (rc == DD_OK) {
+      e = cudaMemcpyAsync(ids, di, nq * k * 4, cudaMemcpyDeviceToHost, h->stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(dists, dd, nq * k * 4, cudaMemcpyDeviceToHost, h->stream);
+      if (e == cudaSuccess && visited) e = cudaMemcpyAsync(visited, dv, nq * 4, cudaMemcpyDeviceToHost, h->stream);
+      if (e == cudaSuccess && cmps) e = cudaMemcpyAsync(cmps, dc, nq * 4, cudaMemcpyDeviceToHost, h->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    }
+  }
+  cudaFree(dq); cudaFree(dL); cudaFree(di); cudaFree(dd); cudaFree(dv); cudaFree(dc);
+  if (rc) return rc;
+  CK(e);
+  return check_error_word(h);
+}
+
+int dd_beam_search(dd_index* h, const void* queries, uint64_t nq, uint64_t qstride,
+                   const int64_t* self_ids, uint32_t L, uint32_t k, double cut, uint64_t limit,
+                   uint32_t degree_limit, uint32_t start, uint32_t vcap, uint32_t* fr_ids,
+                   float* fr_dists, uint32_t* fr_sizes, uint32_t* vis_ids, float* vis_dists,
+                   uint32_t* vis_sizes, uint32_t* cmps) {
+  if (!h || !queries || !self_ids || nq == 0) return DD_ERR_ARG;
+  if (L == 0 || L > kMaxL) return fail(h, DD_ERR_UNSUPPORTED, "L must be in [1, %u]", kMaxL);
+  if (start >= h->n) return fail(h, DD_ERR_ARG, "start point >= n");
+  CK(cudaSetDevice(h->device));
+  uint64_t rb = (uint64_t)h->d * esize(h->dtype), ds = h->stride;
+  WarpLayout lay = make_search_layout(h->d, h->dtype, L, h->Rp, vcap, false);
+  if (lay.total > 227 * 1024) return fail(h, DD_ERR_UNSUPPORTED, "beam shared memory too large");
+  uint8_t* dq = nullptr;
+  int64_t* dself = nullptr;
+  uint32_t *dfi = nullptr, *dfn = nullptr, *dvi = nullptr, *dvn = nullptr, *dcm = nullptr;
+  float *dfd = nullptr, *dvd = nullptr;
+  cudaError_t e = dalloc(&dq, nq * ds);
+  if (e == cudaSuccess) e = dalloc(&dself, nq);
+  if (e == cudaSuccess) e = dalloc(&dfi, nq * L);
+  if (e == cudaSuccess) e = dalloc(&dfd, nq * L);
+  if (e == cudaSuccess) e = dalloc(&dfn, nq);
+  if (e == cudaSuccess) e = dalloc(&dvi, nq * vcap);
+  if (e == cudaSuccess) e = dalloc(&dvd, nq * vcap);
+  if (e == cudaSuccess) e = dalloc(&dvn, nq);
+  if (e == cudaSuccess) e = dalloc(&dcm, nq);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dq, 0, nq * ds, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(dq, ds, queries, qstride, rb, nq, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dself, self_ids, nq * 8, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) {
+    BeamArgs ba;
+    ba.queries = dq; ba.qstride = ds; ba.nq = nq; ba.self_ids = dself; ba.L = L; ba.k = k;
+    ba.cut = cut; ba.limit = limit ? limit : h->n;
+    ba.degree_limit = degree_limit ? std::min(degree_limit, h->R) : h->R;
+    ba.start = start; ba.vcap = vcap;
+    ba.fr_ids = dfi; ba.fr_d = dfd; ba.fr_n = dfn; ba.vis_ids = dvi; ba.vis_d = dvd;
+    ba.vis_n = dvn; ba.cmps = dcm;
+    launch_beam(view(h), ba, lay, h->stream);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(fr_ids, dfi, nq * L * 4, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(fr_dists, dfd, nq * L * 4, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(fr_sizes, dfn, nq * 4, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(vis_ids, dvi, nq * vcap * 4, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(vis_dists, dvd, nq * vcap * 4, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(vis_sizes, dvn, nq * 4, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(cmps, dcm, nq * 4, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  void* fr[] = {dq, dself, dfi, dfd, dfn, dvi, dvd, dvn, dcm};
+  for (void* p : fr) dfree(p);
+  CK(e);
+  return check_error_word(h);
+}
+
+int dd_robust_prune(dd_index* h, uint32_t ntasks, const uint32_t* p, const uint64_t* offsets,
+                    const uint32_t* cand_ids, const float* cand_dists, double alpha,
+                    uint32_t* out, uint32_t* out_len) {
+  if (!h || !p || !offsets || !out || !out_len) return DD_ERR_ARG;
+  if (ntasks == 0) return DD_OK;
+  for (uint32_t t = 0; t < ntasks; t++)
+    if (p[t] >= h->n || offsets[t + 1] < offsets[t]) return fail(h, DD_ERR_ARG, "bad task %u", t);
+  for (uint64_t i = 0; i < offsets[ntasks]; i++)
+    if (cand_ids[i] >= h->n) return fail(h, DD_ERR_ARG, "candidate id %u >= n", cand_ids[i]);
+  CK(cudaSetDevice(h->device));
+  uint64_t tot = offsets[ntasks];
+  uint64_t ws = tot + (uint64_t)ntasks * h->Rp;
+  uint32_t *dp = nullptr, *dci = nullptr, *dout = nullptr, *gc = nullptr;
+  uint64_t* doff = nullptr;
+  float *dcd = nullptr, *gk = nullptr;
+  int* gl = nullptr;
+  cudaError_t e = dalloc(&dp, ntasks);
+  if (e == cudaSuccess) e = dalloc(&doff, ntasks + 1);
+  if (e == cudaSuccess) e = dalloc(&dci, tot);
+  if (e == cudaSuccess) e = dalloc(&dcd, tot);
+  if (e == cudaSuccess) e = dalloc(&dout, (uint64_t)ntasks * h->Rp);
+  if (e == cudaSuccess) e = dalloc(&gc, ws);
+  if (e == cudaSuccess) e = dalloc(&gk, ws);
+  if (e == cudaSuccess) e = dalloc(&gl, 2 * ws + (uint64_t)ntasks * kGlobalStackInts);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dp, p, ntasks * 4, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(doff, offsets, (ntasks + 1) * 8ull, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess && tot) e = cudaMemcpyAsync(dci, cand_ids, tot * 4, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess && tot) e = cudaMemcpyAsync(dcd, cand_dists, tot * 4, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) {
+    PruneArgs pa;
+    pa.ntasks = ntasks; pa.p = dp; pa.offsets = doff; pa.cand_ids = dci; pa.cand_d = dcd;
+    pa.alpha = alpha; pa.out = dout; pa.gcand = gc; pa.gkey = gk; pa.gleaf = gl;
+    launch_prune_tasks(view(h), pa, h->stream);
+    e = cudaGetLastError();
+  }
+  std::vector<uint32_t> o((uint64_t)ntasks * h->Rp);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(o.data(), dout, o.size() * 4, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  void* fr[] = {dp, doff, dci, dcd, dout, gc, gk, gl};
+  for (void* q : fr) dfree(q);
+  CK(e);
+  for (uint32_t t = 0; t < ntasks; t++) {
+    uint32_t len = 0;
+    while (len < h->R && o[(uint64_t)t * h->Rp + len] != DD_NONE) len++;
+    out_len[t] = len;
+    for (uint32_t j = 0; j < h->R; j++) out[(uint64_t)t * h->R + j] = j < len ? o[(uint64_t)t * h->Rp + j] : 0u;
+  }
+  return check_error_word(h);
+}
+
+int dd_groundtruth(dd_index* h, const void* queries, uint64_t nq, uint64_t qstride, uint32_t k,
+                   uint32_t* ids, float* dists) {
+  if (!h || !queries || !ids || !dists) return DD_ERR_ARG;
+  if (k == 0 || k > 32 || k > h->n) return fail(h, DD_ERR_UNSUPPORTED, "k must be in [1, 32]");
+  if (nq == 0) return DD_OK;
+  CK(cudaSetDevice(h->device));
+  uint64_t rb = (uint64_t)h->d * esize(h->dtype), ds = h->stride;
+  uint32_t nchunks = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(256, h->n / 4096));
+  uint8_t* dq = nullptr;
+  uint32_t *di = nullptr, *pi = nullptr;
+  float* dd = nullptr;
+  double* pd = nullptr;
+  cudaError_t e = dalloc(&dq, nq * ds);
+  if (e == cudaSuccess) e = dalloc(&di, nq * k);
+  if (e == cudaSuccess) e = dalloc(&dd, nq * k);
+  if (e == cudaSuccess) e = dalloc(&pi, nq * nchunks * k);
+  if (e == cudaSuccess) e = dalloc(&pd, nq * nchunks * k);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dq, 0, nq * ds, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(dq, ds, queries, qstride, rb, nq, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) {
+    launch_groundtruth(view(h), dq, ds, nq, k, di, dd, pd, pi, nchunks, h->stream);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ids, di, nq * k * 4, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dists, dd, nq * k * 4, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  void* fr[] = {dq, di, dd, pi, pd};
+  for (void* q : fr) dfree(q);
+  CK(e);
+  return DD_OK;
+}
+
+void* dd_device_points(dd_index* h) { return h ? h->points : nullptr; }
+uint64_t dd_device_row_stride(dd_index* h) { return h ? h->stride : 0; }
+void* dd_device_graph(dd_index* h) { return h ? h->graph : nullptr; }
+uint32_t dd_device_row_len(dd_index* h) { return h ? h->Rp : 0; }
+uint64_t dd_last_launch_count(dd_index* h) { return h ? h->launches : 0; }
+
+}  // extern "C"

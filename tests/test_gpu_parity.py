@@ -1,0 +1,186 @@
+"""GPU parity: the CUDA path (through the C ABI) against the reference's own
+outputs (tests/golden/, pinned) and against the CPU oracle on the same seeded
+inputs.  Integer AND float graphs are compared bit-exactly: the kernels
+reproduce the reference's float summation order, its tie orders (std::sort
+emulation) and its lossy hash filter, so no tolerance is needed."""
+import numpy as np
+import pytest
+
+from distributed_diskann_b200 import datasets as D
+from distributed_diskann_b200.index import GpuIndex
+from tests.golden.make_golden import BUILD_CASES, case_inputs, canon, sha
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def need_gpu():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def gpu_build(base, R, L, alpha, metric="l2", **kw):
+    gi = GpuIndex(base.dtype, metric, base.shape[0], base.shape[1], R)
+    gi.upload_points(base)
+    st = gi.build(L, alpha, **kw)
+    return gi, canon(gi.graph()), st
+
+
+@pytest.mark.parametrize("name", list(BUILD_CASES))
+def test_build_and_search_bit_exact_vs_reference(golden, name):
+    g, arrays = golden
+    rec = g["cases"][name]
+    R, L, alpha, metric, xita, mx, st, knn, tp, Ls = BUILD_CASES[name]
+    base, queries = case_inputs(name)
+    gi, graph, stats = gpu_build(base, R, L, alpha, metric=metric, max_fraction=xita, max_build=mx,
+                                 start_point=st, knn_mode=knn, two_pass=tp)
+    if f"{name}__graph" in arrays:
+        np.testing.assert_array_equal(graph, arrays[f"{name}__graph"])
+    assert sha(graph) == rec["graph_sha256"], f"{name}: graph differs from the reference build"
+    for Ls_, s in rec["search"].items():
+        ids, dists, vis, cmps = gi.search(queries, s["k"], int(Ls_), cut=1.35, start=st)
+        assert sha(ids) == s["ids_sha256"], f"{name}: search L={Ls_}"
+        assert int(vis.sum()) == s["visited_sum"]
+        assert int(cmps.sum()) == s["cmps_sum"]
+    gi.close()
+
+
+def test_build_stats_match_oracle(oracle_mod):
+    base, _ = case_inputs("i8_small")
+    gi, graph, st = gpu_build(base, 64, 128, 1.2)
+    og, ost = oracle_mod.build(base, 64, 128, 1.2)
+    np.testing.assert_array_equal(graph, canon(og))
+    assert st["visited"] == ost["visited"]
+    assert st["dist_cmps"] == ost["dist_cmps"]
+    assert st["groups"] == ost["groups"]
+    assert st["reverse_prunes"] == ost["reverse_prunes"]
+    assert st["prune_cands"] == ost["prune_cands"]
+    gi.close()
+
+
+def test_beam_search_frontier_and_visited_vs_reference(golden):
+    g, arrays = golden
+    base, queries = case_inputs("i8_small")
+    gi = GpuIndex(base.dtype, "l2", base.shape[0], base.shape[1], 64)
+    gi.upload_points(base)
+    gi.build(128, 1.2)
+    for mode, (k, L, cut) in {"build": (0, 128, 0.0), "query": (10, 50, 1.35)}.items():
+        res = gi.beam_search(queries[: g["beam_cases"]], L, k=k, cut=cut,
+                             self_ids=np.arange(g["beam_cases"]))
+        for i, (fr, vi, cm) in enumerate(res):
+            np.testing.assert_array_equal(fr[0], arrays[f"beam_{mode}{i}__fr_ids"])
+            np.testing.assert_array_equal(fr[1], arrays[f"beam_{mode}{i}__fr_d"])
+            np.testing.assert_array_equal(vi[0], arrays[f"beam_{mode}{i}__vi_ids"])
+            np.testing.assert_array_equal(vi[1], arrays[f"beam_{mode}{i}__vi_d"])
+            assert cm == int(arrays[f"beam_{mode}{i}__cmps"][0])
+    gi.close()
+
+
+def test_robust_prune_vs_reference(golden):
+    g, arrays = golden
+    base, _ = case_inputs("i8_small")
+    gi = GpuIndex(base.dtype, "l2", base.shape[0], base.shape[1], 64)
+    gi.upload_points(base)
+    gi.build(128, 1.2)
+    tasks = [(int(arrays[f"prune{t}__p"][0]), arrays[f"prune{t}__cand"], arrays[f"prune{t}__dist"])
+             for t in range(g["prune_cases"])]
+    outs = gi.robust_prune(tasks, 1.2)
+    for t, o in enumerate(outs):
+        np.testing.assert_array_equal(o, arrays[f"prune{t}__out"], err_msg=f"prune case {t}")
+    gi.close()
+
+
+@pytest.mark.parametrize("dtype,metric", [("f32", "l2"), ("f32", "mips"), ("i8", "l2"),
+                                          ("u8", "l2"), ("i8", "mips")])
+def test_groundtruth_vs_oracle(oracle_mod, dtype, metric):
+    rng = np.random.default_rng(7)
+    if dtype == "f32":
+        base = rng.standard_normal((20_000, 40), dtype=np.float32)
+        q = rng.standard_normal((300, 40), dtype=np.float32)
+    elif dtype == "i8":
+        base = rng.integers(-128, 128, (20_000, 40)).astype(np.int8)
+        q = rng.integers(-128, 128, (300, 40)).astype(np.int8)
+    else:
+        base = rng.integers(0, 256, (20_000, 40)).astype(np.uint8)
+        q = rng.integers(0, 256, (300, 40)).astype(np.uint8)
+    gi = GpuIndex(base.dtype, metric, base.shape[0], base.shape[1], 8)
+    gi.upload_points(base)
+    ids, ds = gi.groundtruth(q, 32)
+    oi, od = oracle_mod.groundtruth(base, q, 32, metric=metric)
+    np.testing.assert_array_equal(ids, oi)
+    np.testing.assert_array_equal(ds, od)
+    gi.close()
+
+
+def test_mixed_beam_widths_in_one_launch(golden):
+    g, _ = golden
+    base, queries = case_inputs("i8_small")
+    gi = GpuIndex(base.dtype, "l2", base.shape[0], base.shape[1], 64)
+    gi.upload_points(base)
+    gi.build(128, 1.2)
+    Ls = np.array([10, 20, 50, 100, 200], np.uint32)[np.arange(len(queries)) % 5]
+    ids_mixed, _, vis_m, cm_m = gi.search(queries, 10, Ls)
+    for L in (10, 20, 50, 100, 200):
+        ids, _, vis, cm = gi.search(queries, 10, L)
+        sel = Ls == L
+        np.testing.assert_array_equal(ids_mixed[sel], ids[sel])
+        np.testing.assert_array_equal(cm_m[sel], cm[sel])
+    gi.close()
+
+
+def test_graph_file_roundtrip(tmp_path, oracle_mod):
+    base, _ = case_inputs("params_u8")
+    gi, graph, _ = gpu_build(base, 16, 32, 1.2)
+    gi.save_graph(str(tmp_path / "g.bin"))
+    np.testing.assert_array_equal(oracle_mod.read_graph(str(tmp_path / "g.bin")), graph)
+    gi2 = GpuIndex(base.dtype, "l2", base.shape[0], base.shape[1], 16)
+    gi2.upload_points(base)
+    gi2.load_graph(str(tmp_path / "g.bin"))
+    np.testing.assert_array_equal(canon(gi2.graph()), graph)
+    gi.close()
+    gi2.close()
+
+
+@pytest.mark.parametrize("R,L,metric", [(24, 48, "l2"), (64, 96, "l2"), (40, 64, "mips")])
+def test_two_pass_graphs_and_their_queries_vs_oracle(oracle_mod, R, L, metric):
+    """Two-pass builds append reverse edges to rows that may already hold the
+    source, so rows carry duplicate ids and the lossy filter can let one id
+    into a step twice: the frontier and visited lists become multisets."""
+    both = D.gen_mixture_i8(6_300, 50, 100, 13)
+    base, q = both[:6_000], both[6_000:]
+    gi, graph, st = gpu_build(base, R, L, 1.2, metric=metric, two_pass=True)
+    og, ost = oracle_mod.build(base, R, L, 1.2, metric=metric, two_pass=True)
+    np.testing.assert_array_equal(graph, canon(og))
+    assert st["visited"] == ost["visited"] and st["dist_cmps"] == ost["dist_cmps"]
+    for Lq in (10, 50, 128):
+        ids, _, vis, cm = gi.search(q, 10, Lq)
+        oi, ov, oc = oracle_mod.search(base, graph, q, 10, Lq, metric=metric)
+        np.testing.assert_array_equal(ids, oi)
+        np.testing.assert_array_equal(vis, ov)
+        np.testing.assert_array_equal(cm, oc)
+    gi.close()
+
+
+def test_mid_size_int8_build_bit_exact_vs_oracle(oracle_mod):
+    """100k x 100 int8 (the reference's own measured case) against the oracle."""
+    base = D.gen_mixture_i8(100_000, 100, 1000, 4)
+    gi, graph, st = gpu_build(base, 64, 128, 1.2)
+    og, ost = oracle_mod.build(base, 64, 128, 1.2)
+    np.testing.assert_array_equal(graph, canon(og))
+    gi.close()
+
+
+def test_error_word_reports_bad_graph_ids():
+    base = np.zeros((100, 8), np.uint8)
+    gi = GpuIndex(base.dtype, "l2", 100, 8, 4)
+    gi.upload_points(base)
+    bad = np.zeros((100, 5), np.uint32)
+    bad[:, 0] = 1
+    bad[:, 1] = 1000  # out of range
+    from distributed_diskann_b200._lib import DDError
+
+    with pytest.raises(DDError):
+        gi.set_graph(bad)
+    gi.close()
