@@ -1,0 +1,377 @@
+"""Benchmark of the B200 Vamana hot path (batched build + query beam search).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+A step is one full batched (prefix-doubling) build of the workload: beam
+search + robustPrune for every point, then reverse-edge semisort + append /
+prune, round after round.  Default workload: 10,000,000 x 128 uint8 (seeded,
+skewed non-negative values from a 10,000-centre mixture), L2, R=64, L=128,
+alpha=1.2 -- the BIGANN-10M shape.
+
+value : build points/s with the points already resident in HBM (device time,
+        CUDA events, max over ranks).
+e2e   : the same build through the C ABI with host buffers: pinned-host upload
+        of the points, build, download of the graph, all inside the timed region.
+Also reported: the query sweep (L in {10,20,50,100,200}, k=10, recall@10 with
+ties against a GPU brute-force ground truth), the roofline of the dominant
+kernel and the reference's own CPU build timed on a sample.
+
+With N > 1 ranks (torchrun), each rank builds an independent partition of the
+same size (no data-path collective): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "build pts/s; QPS@recall10>=0.95, BF16/INT8+rerank vs exact plain, 1 B200"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="bigann-u8")
+    ap.add_argument("--n", type=int, default=0, help="override the number of base points")
+    ap.add_argument("--nq", type=int, default=0)
+    ap.add_argument("--no-queries", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline work budget")
+    return ap.parse_args()
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    """DRAM bytes per inserted point of the search+prune kernel, from the ncu
+    capture summarised in profiles/ (None if no capture was made)."""
+    p = os.path.join(ROOT, "profiles", "search_prune_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v == "Active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": rows[0][1],
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------- reference CPU arm
+def reference_cpu_build(base, w, budget_s, max_points=2_000_000):
+    """Times the reference's own BSP build (oracle/_ref/ref_harness: the
+    reference sources compiled unmodified) on a leading sample of the workload,
+    sized to about `budget_s` seconds of CPU work.  Returns (pts/s, sample, secs)."""
+    from oracle import oracle as O
+
+    if not os.path.exists(O.REF_HARNESS):
+        raise RuntimeError("reference CPU build missing (oracle/_ref/ref_harness)")
+    cores = os.cpu_count() or 1
+    n = min(20_000, base.shape[0])
+    while True:
+        _, secs = O.ref_build(base[:n], w.R, w.L, w.alpha, metric=w.metric, threads=cores)
+        if secs >= budget_s / 3 or n >= min(max_points, base.shape[0]):
+            return n / secs, n, secs
+        n = int(min(max_points, base.shape[0], n * max(2.0, budget_s / max(secs, 1e-3) / 1.5)))
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    from distributed_diskann_b200 import datasets as D
+
+    w = D.WORKLOADS[args.workload]
+    cores = os.cpu_count() or 1
+    n_total = min(w.n, 2_000_000) if not args.n else args.n
+    base, _ = D.make_workload(w, n=n_total, nq=1)
+    # calibrate one step to a few seconds of CPU work, then W warm-up + K timed steps
+    per_step = max(2.0, min(20.0, 150.0 / max(1, args.warmup + args.steps)))
+    rate, n_s, _ = reference_cpu_build(base, w, per_step)
+    from oracle import oracle as O
+
+    for _ in range(args.warmup):
+        O.ref_build(base[:n_s], w.R, w.L, w.alpha, metric=w.metric, threads=cores)
+    secs = [O.ref_build(base[:n_s], w.R, w.L, w.alpha, metric=w.metric, threads=cores)[1]
+            for _ in range(args.steps)]
+    value = n_s * len(secs) / sum(secs)
+    sample = (f"first {n_s} points of the {w.n}x{w.d} {w.dtype} workload per step "
+              f"(reference BSP build, np=1, PARLAY_NUM_THREADS={cores})")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "points/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * sum(secs) / len(secs), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8" if w.dtype == "u8" else w.dtype,
+        "data": "synthetic",
+        "config": {"workload": f"{w.name} sample", "n": n_s, "d": w.d, "R": w.R, "L": w.L,
+                   "alpha": w.alpha},
+        "cpu_baseline": {"value": value, "unit": "points/s", "cores": cores, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------- our arm
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from distributed_diskann_b200 import datasets as D
+    from distributed_diskann_b200.index import GpuIndex
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    dev = torch.device("cuda", local_rank)
+    w = D.WORKLOADS[args.workload]
+    n = args.n or w.n
+    nq = args.nq or w.nq
+    # each rank builds its own partition (different seed) of the same size
+    import dataclasses
+
+    wr = dataclasses.replace(w, seed=w.seed + 1000 * rank)
+    t0 = time.time()
+    base, queries = D.make_workload(wr, n=n, nq=nq)
+    gen_s = time.time() - t0
+    base_t = torch.from_numpy(base).pin_memory()
+    graph_host = torch.empty((n, w.R + 1), dtype=torch.int32).pin_memory()
+
+    gi = GpuIndex(base.dtype, w.metric, n, w.d, w.R, device=local_rank)
+    stream = torch.cuda.current_stream(dev)
+    gi.set_stream(stream.cuda_stream)
+    gi.upload_points(base)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- warm-up
+    for _ in range(args.warmup):
+        gi.build(w.L, w.alpha, collect_stats=False)
+    barrier()
+
+    # ---- timed builds, inputs resident in HBM
+    gpu_index = os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)).split(",")[local_rank]
+    clocks = ClockSampler(gpu_index)
+    clocks.start()
+    launches = 0
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        gi.build(w.L, w.alpha, collect_stats=False)
+        launches += gi.launches()
+    ev1.record(stream)
+    ev1.synchronize()
+    t_dev = ev0.elapsed_time(ev1) / 1000.0
+    clk = clocks.stop()
+    t_max = max_over_ranks(t_dev)
+    value = world * n * args.steps / t_max
+
+    # ---- e2e through the C ABI with host buffers
+    barrier()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        gi.lib.dd_upload_points(gi.h, base_t.data_ptr(), base_t.stride(0) * base_t.element_size())
+        gi.build(w.L, w.alpha, collect_stats=False)
+        gi.lib.dd_download_graph(gi.h, graph_host.data_ptr())
+    ev1.record(stream)
+    ev1.synchronize()
+    t_e2e = max_over_ranks(ev0.elapsed_time(ev1) / 1000.0)
+    e2e_value = world * n * args.steps / t_e2e
+    h2d = base.nbytes
+    d2h = n * (w.R + 1) * 4
+
+    # ---- one instrumented build: statistics + per-kernel device times
+    st = gi.build(w.L, w.alpha, collect_stats=True)
+    g = gi.graph()
+    deg = g[:, 0]
+    es = 4 if w.dtype == "f32" else 1
+    dsz = w.d * es
+    # algorithmic bytes of the search+prune kernel (per inserted point p):
+    #   V_p*4(R+1) graph rows + C_p*d*s neighbour vectors + d*s own vector
+    #   + |cand_p|*d*s prune candidates + 4R out-list write; |cand_p| = V_p here
+    alg_bytes = (st["visited"] * 4 * (w.R + 1) + st["dist_cmps"] * dsz + n * dsz
+                 + st["visited"] * dsz + n * 4 * w.R)
+    peak, peak_kind = load_peaks()
+    sp_s = st["search_prune_ms"] / 1000.0
+    achieved = alg_bytes / sp_s / 1e9
+    n_launch = st["rounds"]
+    tr = load_traffic()
+    traffic = None
+    if tr:
+        traffic = tr["dram_bytes_per_point"] * n / n_launch
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "kernel": "k_search_prune (fused beam search + robustPrune)",
+                "alg_bytes_per_launch": alg_bytes / n_launch, "launches": n_launch,
+                "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"}
+
+    # ---- queries: GPU ground truth, sweep of beam widths, one mixed-L launch
+    qres = None
+    if not args.no_queries and rank == 0:
+        k = 10
+        gt_i, gt_d = gi.groundtruth(queries, 32)
+        tdt = {"u8": torch.uint8, "i8": torch.int8, "f32": torch.float32}[w.dtype]
+        row_elems = int(gi.lib.dd_device_row_stride(gi.h)) // es
+        qpad = torch.zeros((nq, row_elems), dtype=tdt, device=dev)  # padded device rows
+        qpad[:, : w.d] = torch.from_numpy(queries).to(dev)
+        qstride = qpad.stride(0) * qpad.element_size()
+        ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
+        dd = torch.empty((nq, k), dtype=torch.float32, device=dev)
+        sweep = []
+        for L in w.sweep_L:
+            Ls = torch.full((nq,), L, dtype=torch.int32, device=dev)
+            for _ in range(2):  # first run warms up; the second is timed (checkRecall)
+                barrier()
+                ev0.record(stream)
+                gi.search_device(qpad.data_ptr(), nq, qstride, Ls.data_ptr(), L, k,
+                                 ids.data_ptr(), dd.data_ptr())
+                ev1.record(stream)
+                ev1.synchronize()
+            t = ev0.elapsed_time(ev1) / 1000.0
+            rec = D.recall_with_ties(ids.cpu().numpy().astype(np.uint32), gt_i, gt_d, k)
+            sweep.append({"L": L, "qps": nq / t, "recall10": rec})
+        Ls = torch.tensor(np.array(w.sweep_L, np.int32)[np.arange(nq) % len(w.sweep_L)],
+                          device=dev)
+        barrier()
+        ev0.record(stream)
+        gi.search_device(qpad.data_ptr(), nq, qstride, Ls.data_ptr(), max(w.sweep_L), k,
+                         ids.data_ptr(), dd.data_ptr())
+        ev1.record(stream)
+        ev1.synchronize()
+        mixed_qps = nq / (ev0.elapsed_time(ev1) / 1000.0)
+        ok = [s for s in sweep if s["recall10"] >= 0.95]
+        qres = {"sweep": sweep, "mixed_L_qps": mixed_qps,
+                "qps_at_recall10_0.95": max(s["qps"] for s in ok) if ok else None,
+                "nq": nq, "k": k, "cut": 1.35}
+
+    # ---- CPU baseline: the reference's own build on a sample, rank 0, N = 1
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            rate, n_s, secs = reference_cpu_build(base, w, args.cpu_seconds)
+            cpu = {"value": rate, "unit": "points/s", "cores": os.cpu_count(),
+                   "kind": "reference",
+                   "sample": f"first {n_s} of the {n} points ({secs:.1f} s reference BSP build, "
+                             f"PARLAY_NUM_THREADS={os.cpu_count()})"}
+        except Exception as e:  # reported, never fatal for the GPU numbers
+            cpu = {"value": None, "unit": "points/s", "cores": os.cpu_count(),
+                   "kind": "reference", "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": w.dtype, "data": "synthetic",
+            "config": {"workload": f"{w.name}: {n}x{w.d} {w.dtype} {w.metric}, R={w.R}, "
+                                   f"L={w.L}, alpha={w.alpha} (full batched build per step)",
+                       "n": n, "d": w.d, "R": w.R, "L": w.L, "alpha": w.alpha,
+                       "form": "plain exact (bit-exact vs the reference build)",
+                       "l2_flush": "inputs larger than L2 (points + graph > 126 MB)",
+                       "parallelism": f"{world} independent partitions" if world > 1 else "1 GPU"},
+            "e2e": {"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "build_stats": {k2: st[k2] for k2 in ("rounds", "visited", "dist_cmps", "groups",
+                                                 "reverse_prunes", "prune_cands", "big_groups",
+                                                 "build_ms", "search_prune_ms", "reverse_ms")},
+            "graph": {"avg_degree": float(deg.mean()), "max_degree": int(deg.max())},
+            "queries": qres,
+            "setup_s": {"datagen": gen_s},
+        }
+        print(json.dumps(line), flush=True)
+    gi.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -214,9 +214,35 @@ __global__ void k_accumulate(const uint32_t* stat_vis, const uint32_t* stat_cmps
   }
 }
 
+// Per-round phase events (search+prune kernel, reverse-edge kernels), read once
+// at the end of the build so the rounds run back to back without host syncs.
+struct PhaseEvents {
+  std::vector<cudaEvent_t> ev;
+  size_t used = 0;
+  cudaEvent_t next() {
+    if (used == ev.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      ev.push_back(e);
+    }
+    return ev[used++];
+  }
+  void sum(float* t_search, float* t_rev) {
+    for (size_t i = 0; i + 2 < used; i += 3) {
+      float a = 0, b = 0;
+      cudaEventElapsedTime(&a, ev[i], ev[i + 1]);
+      cudaEventElapsedTime(&b, ev[i + 1], ev[i + 2]);
+      *t_search += a;
+      *t_rev += b;
+    }
+  }
+  ~PhaseEvents() {
+    for (auto e : ev) cudaEventDestroy(e);
+  }
+};
+
 int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& rounds, double alpha,
-                const dd_build_params* P, const WarpLayout& lay, int grid_max, cudaEvent_t* ev,
-                float* t_search, float* t_rev) {
+                const dd_build_params* P, const WarpLayout& lay, int grid_max, PhaseEvents* pe) {
   IndexView ix = view(h);
   for (auto& rd : rounds) {
     uint64_t B = rd.second > rd.first ? rd.second - rd.first : 0;
@@ -231,12 +257,12 @@ int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& r
     ra.stat_vis = h->stat_vis;
     ra.stat_cmps = h->stat_cmps;
     CK(cudaMemsetAsync(h->counters, 0, 8 * 4, h->stream));
-    if (ev) CK(cudaEventRecord(ev[0], h->stream));
+    if (pe) CK(cudaEventRecord(pe->next(), h->stream));
     int grid = (int)std::min<uint64_t>((B + kSearchWarpsPerCta - 1) / kSearchWarpsPerCta,
                                        (uint64_t)grid_max);
     launch_search_prune(ix, ra, lay, kSearchWarpsPerCta, grid, h->stream);
+    if (pe) CK(cudaEventRecord(pe->next(), h->stream));
     launch_apply_rows(ix, ra, h->stream);
-    if (ev) CK(cudaEventRecord(ev[1], h->stream));
     launch_reverse(ix, ra, make_rs(h), h->stream, h->sm_count);
     launch_reverse_big(ix, ra, make_rs(h), kBigSlots, h->stream);
     h->launches += 9;
@@ -245,15 +271,7 @@ int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& r
                                               h->acc);
       h->launches++;
     }
-    if (ev) {
-      CK(cudaEventRecord(ev[2], h->stream));
-      CK(cudaEventSynchronize(ev[2]));
-      float a = 0, b = 0;
-      cudaEventElapsedTime(&a, ev[0], ev[1]);
-      cudaEventElapsedTime(&b, ev[1], ev[2]);
-      *t_search += a;
-      *t_rev += b;
-    }
+    if (pe) CK(cudaEventRecord(pe->next(), h->stream));
     CK(cudaGetLastError());
   }
   return DD_OK;
@@ -463,21 +481,20 @@ int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
   CK(cudaMemsetAsync(h->graph, 0xff, h->n * h->Rp * 4ull, h->stream));
   CK(cudaMemsetAsync(h->acc, 0, 8 * 8, h->stream));
   CK(cudaMemsetAsync(h->err, 0, 4, h->stream));
-  cudaEvent_t e0, e1, ev[3];
+  cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  bool timed = stats != nullptr;
-  for (auto& e : ev) CK(cudaEventCreate(&e));
+  PhaseEvents pe;
+  PhaseEvents* pep = stats ? &pe : nullptr;
   CK(cudaEventRecord(e0, h->stream));
   float ts = 0, tr = 0;
-  // RoundArgs fields that depend on the pass are set inside pass_rounds
   dd_build_params Q = *P;
   Q.start_point = start;
   if (P->two_pass) {
-    rc = pass_rounds(h, rounds, 1.0, &Q, lay, grid_max, timed ? ev : nullptr, &ts, &tr);
+    rc = pass_rounds(h, rounds, 1.0, &Q, lay, grid_max, pep);
     if (rc) return rc;
   }
-  rc = pass_rounds(h, rounds, P->alpha, &Q, lay, grid_max, timed ? ev : nullptr, &ts, &tr);
+  rc = pass_rounds(h, rounds, P->alpha, &Q, lay, grid_max, pep);
   if (rc) return rc;
   if (P->knn_mode) {
     launch_sort_rows(view(h), h->stream);
@@ -490,6 +507,7 @@ int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
   if (stats) {
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
+    pe.sum(&ts, &tr);
     unsigned long long acc[8] = {0};
     cudaMemcpy(acc, h->acc, sizeof acc, cudaMemcpyDeviceToHost);
     std::memset(stats, 0, sizeof *stats);
@@ -506,7 +524,6 @@ int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  for (auto& e : ev) cudaEventDestroy(e);
   return rc;
 }
 
