@@ -13,6 +13,7 @@
 #include "../../include/dd_gpu.h"
 #include "dd_common.cuh"
 #include "kernels.cuh"
+#include "semisort.cuh"
 #include "sort_emul.cuh"
 
 using namespace ddk;
@@ -35,24 +36,29 @@ struct dd_index {
   uint32_t* new_out = nullptr;
   uint32_t* stat_vis = nullptr;
   uint32_t* stat_cmps = nullptr;
-  uint32_t* keys = nullptr;
-  uint32_t* cnt = nullptr;
-  uint32_t* cursor = nullptr;
-  uint32_t* touched = nullptr;
-  uint32_t* seg_start = nullptr;
+  uint32_t* sort_t[2] = {nullptr, nullptr};  // semisort ping-pong buffers
+  uint32_t* sort_v[2] = {nullptr, nullptr};
+  uint32_t* hist = nullptr;
+  uint32_t* heads = nullptr;
+  uint32_t* flags = nullptr;
   uint32_t* counters = nullptr;
   uint32_t* big = nullptr;
   uint32_t* block_sums = nullptr;
   unsigned long long* acc = nullptr;  // [0] visited [1] cmps [2] groups [3] prunes [4] cands [5] big
-  uint32_t* gcand = nullptr;
+  uint32_t* gcand = nullptr;          // CTA big-target workspace slices
   float* gkey = nullptr;
-  int* gleaf = nullptr;
+  int* gpos = nullptr;
+  uint32_t* gbits = nullptr;
+  int* granges = nullptr;
   uint64_t gcap = 0;
+  // per-warp visited-list slices of the build searches (grown on demand)
+  uint32_t* hash_arena = nullptr;
+  uint64_t hash_arena_words = 0;
+  bool verbose = false;
 };
 
 namespace {
 
-constexpr uint32_t kBigSlots = 16;
 constexpr int kSearchWarpsPerCta = 2;
 
 int fail(dd_index* h, int code, const char* fmt, ...) {
@@ -144,49 +150,77 @@ std::vector<std::pair<uint64_t, uint64_t>> schedule(uint64_t n, uint64_t max_bui
 }
 
 int ensure_build_scratch(dd_index* h, uint64_t B) {
-  if (!h->cnt) {
-    CK(dalloc(&h->cnt, h->n));
-    CK(dalloc(&h->cursor, h->n));
-    CK(cudaMemsetAsync(h->cnt, 0, h->n * 4, h->stream));
+  if (!h->counters) {
     CK(dalloc(&h->counters, 8));
     CK(dalloc(&h->block_sums, kScanBlocks + 1));
     CK(dalloc(&h->acc, 8));
   }
   if (B <= h->bcap) return DD_OK;
-  dfree(h->new_out); dfree(h->stat_vis); dfree(h->stat_cmps); dfree(h->keys);
-  dfree(h->touched); dfree(h->seg_start); dfree(h->big);
-  dfree(h->gcand); dfree(h->gkey); dfree(h->gleaf);
-  uint64_t E = B * h->Rp;
-  uint64_t T = std::min<uint64_t>(h->n, E);
+  void* old[] = {h->new_out, h->stat_vis, h->stat_cmps, h->sort_t[0], h->sort_t[1], h->sort_v[0],
+                 h->sort_v[1], h->hist, h->heads, h->flags, h->big, h->gcand, h->gkey,
+                 h->gpos, h->gbits, h->granges};
+  for (void* p : old) dfree(p);
+  const uint64_t E = B * h->Rp;
   CK(dalloc(&h->new_out, E));
   CK(dalloc(&h->stat_vis, B));
   CK(dalloc(&h->stat_cmps, B));
-  CK(dalloc(&h->keys, E));
-  CK(dalloc(&h->touched, T));
-  CK(dalloc(&h->seg_start, T));
-  CK(dalloc(&h->big, T));
+  for (int i = 0; i < 2; i++) {
+    CK(dalloc(&h->sort_t[i], E));
+    CK(dalloc(&h->sort_v[i], E));
+  }
+  CK(dalloc(&h->hist, semisort_hist_words(E)));
+  CK(dalloc(&h->heads, E));
+  CK(dalloc(&h->flags, E));
+  CK(dalloc(&h->big, E));
   h->gcap = B + h->Rp;
   CK(dalloc(&h->gcand, kBigSlots * h->gcap));
   CK(dalloc(&h->gkey, kBigSlots * h->gcap));
-  CK(dalloc(&h->gleaf, kBigSlots * (2 * h->gcap + ddsort::stack_ints((int)h->gcap))));
+  CK(dalloc(&h->gpos, kBigSlots * 2 * h->gcap));
+  CK(dalloc(&h->gbits, kBigSlots * (h->gcap / 32 + 2)));
+  CK(dalloc(&h->granges, kBigSlots * 3 * (h->gcap / 8 + 64)));
   h->bcap = B;
   return DD_OK;
 }
 
-// the reverse-edge scratch of a handle
-ReverseScratch make_rs(dd_index* h) {
+SemisortScratch make_ss(dd_index* h) {
+  SemisortScratch s;
+  for (int i = 0; i < 2; i++) {
+    s.t[i] = h->sort_t[i];
+    s.v[i] = h->sort_v[i];
+  }
+  s.hist = h->hist;
+  s.heads = h->heads;
+  s.flags = h->flags;
+  s.block_sums = h->block_sums;
+  s.counters = h->counters;
+  s.cap = h->bcap * h->Rp;
+  return s;
+}
+
+// room for `words` uint32 of per-warp hash tables
+int ensure_hash_arena(dd_index* h, uint64_t words) {
+  if (words <= h->hash_arena_words) return DD_OK;
+  dfree(h->hash_arena);
+  h->hash_arena = nullptr;
+  h->hash_arena_words = 0;
+  CK(dalloc(&h->hash_arena, words));
+  h->hash_arena_words = words;
+  return DD_OK;
+}
+
+// the reverse-edge scratch of a handle; `res` = semisort result buffer
+ReverseScratch make_rs(dd_index* h, int res) {
   ReverseScratch rs;
-  rs.cnt = h->cnt;
-  rs.cursor = h->cursor;
-  rs.touched = h->touched;
-  rs.seg_start = h->seg_start;
-  rs.keys = h->keys;
+  rs.st = h->sort_t[res];
+  rs.sv = h->sort_v[res];
+  rs.heads = h->heads;
   rs.counters = h->counters;
   rs.big = h->big;
-  rs.block_sums = h->block_sums;
   rs.gcand = h->gcand;
   rs.gkey = h->gkey;
-  rs.gleaf = h->gleaf;
+  rs.gpos = h->gpos;
+  rs.gbits = h->gbits;
+  rs.granges = h->granges;
   rs.gcap = h->gcap;
   return rs;
 }
@@ -207,10 +241,10 @@ __global__ void k_accumulate(const uint32_t* stat_vis, const uint32_t* stat_cmps
     atomicAdd(&acc[1], sc);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    atomicAdd(&acc[2], (unsigned long long)counters[0]);
+    atomicAdd(&acc[2], (unsigned long long)counters[1]);
     atomicAdd(&acc[3], (unsigned long long)counters[2]);
     atomicAdd(&acc[4], (unsigned long long)counters[3]);
-    atomicAdd(&acc[5], (unsigned long long)counters[1]);
+    atomicAdd(&acc[5], (unsigned long long)counters[4]);
   }
 }
 
@@ -256,6 +290,7 @@ int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& r
     ra.new_out = h->new_out;
     ra.stat_vis = h->stat_vis;
     ra.stat_cmps = h->stat_cmps;
+    ra.vis_arena = h->hash_arena;
     CK(cudaMemsetAsync(h->counters, 0, 8 * 4, h->stream));
     if (pe) CK(cudaEventRecord(pe->next(), h->stream));
     int grid = (int)std::min<uint64_t>((B + kSearchWarpsPerCta - 1) / kSearchWarpsPerCta,
@@ -263,9 +298,10 @@ int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& r
     launch_search_prune(ix, ra, lay, kSearchWarpsPerCta, grid, h->stream);
     if (pe) CK(cudaEventRecord(pe->next(), h->stream));
     launch_apply_rows(ix, ra, h->stream);
-    launch_reverse(ix, ra, make_rs(h), h->stream, h->sm_count);
-    launch_reverse_big(ix, ra, make_rs(h), kBigSlots, h->stream);
-    h->launches += 9;
+    SemisortScratch ss = make_ss(h);
+    const int res = launch_semisort(h->new_out, B * h->Rp, h->n, ss, h->stream);
+    launch_reverse(ix, ra, make_rs(h, res), h->stream, h->sm_count);
+    h->launches += 6 + 5 * (uint64_t)((64 - __builtin_clzll(h->n > 1 ? h->n - 1 : 1) + 7) / 8);
     if (P->collect_stats) {
       k_accumulate<<<64, 256, 0, h->stream>>>(h->stat_vis, h->stat_cmps, (uint32_t)B, h->counters,
                                               h->acc);
@@ -273,6 +309,16 @@ int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& r
     }
     if (pe) CK(cudaEventRecord(pe->next(), h->stream));
     CK(cudaGetLastError());
+    if (h->verbose) {  // per-round diagnostics (DD_VERBOSE=1): synchronizes every round
+      uint32_t c[8];
+      CK(cudaMemcpyAsync(c, h->counters, sizeof c, cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+      fprintf(stderr,
+              "[dd] round [%llu, %llu) B=%llu pairs=%u targets=%u pruned=%u cands=%u big=%u "
+              "max_big=%u\n",
+              (unsigned long long)rd.first, (unsigned long long)rd.second, (unsigned long long)B,
+              c[0], c[1], c[2], c[3], c[4], c[5]);
+    }
   }
   return DD_OK;
 }
@@ -299,6 +345,10 @@ int dd_create(int dtype, int metric, uint64_t n, uint32_t d, uint32_t R, int dev
   h->Rp = (R + 3) & ~3u;
   h->stride = ((uint64_t)d * esize(dtype) + 63) & ~(uint64_t)63;
   h->device = device;
+  {
+    const char* v = getenv("DD_VERBOSE");
+    h->verbose = v && v[0] == '1';
+  }
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) e = cudaMalloc((void**)&h->points, n * h->stride);
@@ -320,9 +370,10 @@ int dd_create(int dtype, int metric, uint64_t n, uint32_t d, uint32_t R, int dev
 int dd_destroy(dd_index* h) {
   if (!h) return DD_OK;
   cudaSetDevice(h->device);
-  void* ptrs[] = {h->points, h->graph, h->err, h->new_out, h->stat_vis, h->stat_cmps, h->keys,
-                  h->cnt, h->cursor, h->touched, h->seg_start, h->counters, h->big,
-                  h->block_sums, h->acc, h->gcand, h->gkey, h->gleaf};
+  void* ptrs[] = {h->points, h->graph, h->err, h->new_out, h->stat_vis, h->stat_cmps,
+                  h->sort_t[0], h->sort_t[1], h->sort_v[0], h->sort_v[1], h->hist, h->heads,
+                  h->flags, h->counters, h->big, h->block_sums, h->acc, h->gcand, h->gkey,
+                  h->gpos, h->gbits, h->granges, h->hash_arena};
   for (void* p : ptrs) dfree(p);
   delete h;
   return DD_OK;
@@ -470,12 +521,10 @@ int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
   WarpLayout lay = make_search_layout(h->d, h->dtype, P->L, h->Rp, vcap, true);
   if ((size_t)lay.total * kSearchWarpsPerCta > 227 * 1024)
     return fail(h, DD_ERR_UNSUPPORTED, "per-warp shared memory %u B too large (L=%u)", lay.total, P->L);
-  int bps = 1;
-  {
-    size_t sm = (size_t)lay.total * kSearchWarpsPerCta;
-    bps = std::max(1, (int)((228 * 1024) / (sm + 1024)));
-  }
-  int grid_max = bps * h->sm_count;
+  const int bps = search_blocks_per_sm(view(h), lay, P->L, kSearchWarpsPerCta, true);
+  const int grid_max = bps * h->sm_count;
+  rc = ensure_hash_arena(h, (uint64_t)grid_max * kSearchWarpsPerCta * 2ull * lay.vcap);
+  if (rc) return rc;
 
   // empty graph (the reference starts from Graph(R, n): all degrees 0)
   CK(cudaMemsetAsync(h->graph, 0xff, h->n * h->Rp * 4ull, h->stream));
@@ -544,9 +593,8 @@ int dd_search_device(dd_index* h, const void* queries, uint64_t nq, uint64_t qst
   while (wpc > 1 && (size_t)lay.total * wpc > 227 * 1024) wpc >>= 1;
   if ((size_t)lay.total * wpc > 227 * 1024)
     return fail(h, DD_ERR_UNSUPPORTED, "query shared memory %u B too large", lay.total);
-  size_t sm = (size_t)lay.total * wpc;
-  int bps = std::max(1, (int)((228 * 1024) / (sm + 1024)));
-  int grid = (int)std::min<uint64_t>((nq + wpc - 1) / wpc, (uint64_t)bps * h->sm_count);
+  const int bps = search_blocks_per_sm(view(h), lay, Lmax, wpc, false);
+  const int grid = (int)std::min<uint64_t>((nq + wpc - 1) / wpc, (uint64_t)bps * h->sm_count);
   QueryArgs qa;
   qa.queries = (const uint8_t*)queries;
   qa.qstride = qstride;
@@ -623,6 +671,7 @@ int dd_beam_search(dd_index* h, const void* queries, uint64_t nq, uint64_t qstri
   uint64_t rb = (uint64_t)h->d * esize(h->dtype), ds = h->stride;
   WarpLayout lay = make_search_layout(h->d, h->dtype, L, h->Rp, vcap, false);
   if (lay.total > 227 * 1024) return fail(h, DD_ERR_UNSUPPORTED, "beam shared memory too large");
+  const int bgrid = (int)std::min<uint64_t>(nq, 4096);
   uint8_t* dq = nullptr;
   int64_t* dself = nullptr;
   uint32_t *dfi = nullptr, *dfn = nullptr, *dvi = nullptr, *dvn = nullptr, *dcm = nullptr;
@@ -648,7 +697,7 @@ int dd_beam_search(dd_index* h, const void* queries, uint64_t nq, uint64_t qstri
     ba.start = start; ba.vcap = vcap;
     ba.fr_ids = dfi; ba.fr_d = dfd; ba.fr_n = dfn; ba.vis_ids = dvi; ba.vis_d = dvd;
     ba.vis_n = dvn; ba.cmps = dcm;
-    launch_beam(view(h), ba, lay, h->stream);
+    launch_beam(view(h), ba, lay, bgrid, h->stream);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(fr_ids, dfi, nq * L * 4, cudaMemcpyDeviceToHost, h->stream);
@@ -688,7 +737,7 @@ int dd_robust_prune(dd_index* h, uint32_t ntasks, const uint32_t* p, const uint6
   if (e == cudaSuccess) e = dalloc(&dout, (uint64_t)ntasks * h->Rp);
   if (e == cudaSuccess) e = dalloc(&gc, ws);
   if (e == cudaSuccess) e = dalloc(&gk, ws);
-  if (e == cudaSuccess) e = dalloc(&gl, 2 * ws + (uint64_t)ntasks * kGlobalStackInts);
+  if (e == cudaSuccess) e = dalloc(&gl, 3 * ws + (uint64_t)ntasks * kGlobalStackInts);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dp, p, ntasks * 4, cudaMemcpyHostToDevice, h->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(doff, offsets, (ntasks + 1) * 8ull, cudaMemcpyHostToDevice, h->stream);
   if (e == cudaSuccess && tot) e = cudaMemcpyAsync(dci, cand_ids, tot * 4, cudaMemcpyHostToDevice, h->stream);
@@ -696,7 +745,7 @@ int dd_robust_prune(dd_index* h, uint32_t ntasks, const uint32_t* p, const uint6
   if (e == cudaSuccess) {
     PruneArgs pa;
     pa.ntasks = ntasks; pa.p = dp; pa.offsets = doff; pa.cand_ids = dci; pa.cand_d = dcd;
-    pa.alpha = alpha; pa.out = dout; pa.gcand = gc; pa.gkey = gk; pa.gleaf = gl;
+    pa.alpha = alpha; pa.out = dout; pa.gcand = gc; pa.gkey = gk; pa.gws = gl;
     launch_prune_tasks(view(h), pa, h->stream);
     e = cudaGetLastError();
   }

@@ -190,6 +190,100 @@ template <> struct Dist<DD_U8, DD_MIPS> : DistIntIP<DD_U8> {};
 template <int DT>
 struct ElemSize { static constexpr int v = (DT == DD_F32) ? 4 : 1; };
 
+// Distances from `a` to up to C rows at once (row t used when act[t]); the
+// loads of the C rows are interleaved so their latencies overlap.  Each row's
+// arithmetic is exactly Dist<DT, MT>::eval's.
+template <int DT, int MT, int C>
+struct DistRows {
+  static __device__ __forceinline__ void eval(const void* av, const uint8_t* const* rows,
+                                              const bool* act, uint32_t d, float* out) {
+    if (DT == DD_F32) {
+      const float* a = (const float*)av;
+      float r[C];
+#pragma unroll
+      for (int t = 0; t < C; t++) r[t] = 0.f;
+      uint32_t i = 0;
+      for (; i + 3 < d; i += 4) {
+        float4 x = *(const float4*)(a + i);
+        float4 y[C];
+#pragma unroll
+        for (int t = 0; t < C; t++)
+          if (act[t]) y[t] = __ldg((const float4*)rows[t] + (i >> 2));
+#pragma unroll
+        for (int t = 0; t < C; t++) {
+          if (!act[t]) continue;
+          if (MT == DD_L2) {
+            float d0 = __fsub_rn(x.x, y[t].x), d1 = __fsub_rn(x.y, y[t].y);
+            float d2 = __fsub_rn(x.z, y[t].z), d3 = __fsub_rn(x.w, y[t].w);
+            float s = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)),
+                                          __fmul_rn(d2, d2)),
+                                __fmul_rn(d3, d3));
+            r[t] = __fadd_rn(r[t], s);
+          } else {
+            r[t] = __fadd_rn(r[t], __fmul_rn(x.x, y[t].x));
+            r[t] = __fadd_rn(r[t], __fmul_rn(x.y, y[t].y));
+            r[t] = __fadd_rn(r[t], __fmul_rn(x.z, y[t].z));
+            r[t] = __fadd_rn(r[t], __fmul_rn(x.w, y[t].w));
+          }
+        }
+      }
+      for (; i < d; i++) {
+#pragma unroll
+        for (int t = 0; t < C; t++) {
+          if (!act[t]) continue;
+          float yv = __ldg((const float*)rows[t] + i);
+          if (MT == DD_L2) {
+            float d0 = __fsub_rn(a[i], yv);
+            r[t] = __fadd_rn(r[t], __fmul_rn(d0, d0));
+          } else {
+            r[t] = __fadd_rn(r[t], __fmul_rn(a[i], yv));
+          }
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < C; t++) out[t] = (MT == DD_L2) ? r[t] : -r[t];
+    } else {
+      const uint4* a = (const uint4*)av;
+      uint32_t nv = (d + 15) >> 4;
+      int acc[C];
+#pragma unroll
+      for (int t = 0; t < C; t++) acc[t] = 0;
+      for (uint32_t i = 0; i < nv; i++) {
+        uint4 x = a[i];
+        uint4 y[C];
+#pragma unroll
+        for (int t = 0; t < C; t++)
+          if (act[t]) y[t] = __ldg((const uint4*)rows[t] + i);
+#pragma unroll
+        for (int t = 0; t < C; t++) {
+          if (!act[t]) continue;
+          if (MT == DD_L2) {
+            uint32_t u = (uint32_t)acc[t], s;
+            s = absdiff4<DT>(x.x, y[t].x); u = __dp4a(s, s, u);
+            s = absdiff4<DT>(x.y, y[t].y); u = __dp4a(s, s, u);
+            s = absdiff4<DT>(x.z, y[t].z); u = __dp4a(s, s, u);
+            s = absdiff4<DT>(x.w, y[t].w); u = __dp4a(s, s, u);
+            acc[t] = (int)u;
+          } else if (DT == DD_U8) {
+            uint32_t u = (uint32_t)acc[t];
+            u = __dp4a(x.x, y[t].x, u); u = __dp4a(x.y, y[t].y, u);
+            u = __dp4a(x.z, y[t].z, u); u = __dp4a(x.w, y[t].w, u);
+            acc[t] = (int)u;
+          } else {
+            int v = acc[t];
+            v = __dp4a((int)x.x, (int)y[t].x, v); v = __dp4a((int)x.y, (int)y[t].y, v);
+            v = __dp4a((int)x.z, (int)y[t].z, v); v = __dp4a((int)x.w, (int)y[t].w, v);
+            acc[t] = v;
+          }
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < C; t++)
+        out[t] = (MT == DD_L2) ? __int2float_rn(acc[t]) : -__int2float_rn(acc[t]);
+    }
+  }
+};
+
 // splitmix64 finaliser: the reference's lossy "seen" filter hashes ids with it
 // (include/utils/beamSearch.h:66-73, include/parlay/utilities.h:145-150).
 __device__ __forceinline__ uint64_t dd_hash64(uint64_t x) {
@@ -204,3 +298,28 @@ __device__ __forceinline__ bool pair_less(float da, uint32_t ia, float db, uint3
 }
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
+
+// CTA-wide exclusive scan (all threads of the block call it; sh: 32 words)
+__device__ __forceinline__ uint32_t cta_scan_excl(uint32_t v, uint32_t* total, uint32_t* sh) {
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  uint32_t x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  if (lane == 31) sh[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    uint32_t s = lane < nw ? sh[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= (uint32_t)o) s += y;
+    }
+    if (lane < nw) sh[lane] = s;
+  }
+  __syncthreads();
+  uint32_t wb = w ? sh[w - 1] : 0;
+  *total = sh[nw - 1];
+  __syncthreads();
+  return wb + x - v;
+}

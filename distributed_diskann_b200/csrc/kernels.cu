@@ -8,7 +8,9 @@
 //                    them by target keeping batch order inside a target
 //                    (src/bsp_index.hpp:362-376, parlay group_by_key)
 //   k_reverse      : one warp per target: append, or robustPrune when the row
-//                    would overflow R (src/bsp_index.hpp:384-407)
+//                    would overflow R (src/bsp_index.hpp:384-407); targets with
+//                    more candidates go to k_reverse_big (one CTA, shared
+//                    memory) or, beyond that, k_reverse_huge (global memory)
 //   k_query        : searchAll (include/utils/beamSearch.h:314-346), mixed L
 //   k_gt_*         : brute-force ground truth (FP64 for float data)
 #include <cfloat>
@@ -22,8 +24,16 @@
 
 namespace ddk {
 
-static __host__ __device__ inline uint32_t r16(uint64_t x) { return (uint32_t)((x + 15) & ~(uint64_t)15); }
+static __host__ __device__ inline uint32_t r16(uint64_t x) {
+  return (uint32_t)((x + 15) & ~(uint64_t)15);
+}
 
+// Per-warp shared memory:
+//   build (with_prune): qv | frontier | step candidates | hash table, where the
+//     hash region is reused after the search as the prune workspace (visited
+//     list + out-list candidates, leaf bitmap, stack); the visited list is
+//     appended to a per-warp global slice during the search.
+//   query / debug: qv | frontier | step candidates | visited (debug) | evicted | hash.
 WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, uint32_t vcap,
                               bool with_prune) {
   WarpLayout w{};
@@ -38,17 +48,19 @@ WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, ui
   w.s_d = off; off += r16(4ull * Rp);
   w.vcap = vcap;
   w.ccap = vcap + Rp;
-  w.vis_id = off; off += r16(4ull * w.ccap);
-  w.vis_d = off; off += r16(4ull * w.ccap);
   w.hbits = hash_bits_for(L);
-  w.ws = off;
-  uint32_t hash_bytes = 4u << w.hbits;
-  uint32_t ev_bytes = r16(4ull * vcap);
-  uint32_t search_ws = hash_bytes + ev_bytes;
-  uint32_t prune_ws = 0;
-  if (with_prune)
-    prune_ws = r16(4ull * w.ccap) * 2 + r16(4ull * ddsort::stack_ints((int)w.ccap)) + 16;
-  off += search_ws > prune_ws ? search_ws : prune_ws;
+  const uint32_t hash_bytes = 4u << w.hbits;
+  if (with_prune) {
+    w.vis_id = w.vis_d = 0;  // global
+    w.ws = off;
+    uint32_t pws = r16(4ull * w.ccap) * 2 + prune_ws_bytes(w.ccap);
+    off += hash_bytes > pws ? hash_bytes : pws;
+  } else {
+    w.vis_id = off; off += r16(4ull * vcap);
+    w.vis_d = off; off += r16(4ull * vcap);
+    w.ws = off; off += r16(4ull * vcap);  // evicted list
+    off += hash_bytes;
+  }
   w.total = r16(off);
   return w;
 }
@@ -58,7 +70,29 @@ struct WarpPtrs {
   PruneSmem Pm;
 };
 
-__device__ __forceinline__ WarpPtrs carve(uint8_t* base, const WarpLayout& w) {
+// build layout: visited list in the global slice vis_g (vcap ids then vcap dists)
+__device__ __forceinline__ WarpPtrs carve_build(uint8_t* base, const WarpLayout& w, uint32_t* vis_g) {
+  WarpPtrs r;
+  r.S.qv = base + w.qv;
+  r.S.fr_id = (uint32_t*)(base + w.fr_id);
+  r.S.fr_d = (float*)(base + w.fr_d);
+  r.S.c_id = (uint32_t*)(base + w.c_id);
+  r.S.c_d = (float*)(base + w.c_d);
+  r.S.s_id = (uint32_t*)(base + w.s_id);
+  r.S.s_d = (float*)(base + w.s_d);
+  r.S.vis_id = vis_g;
+  r.S.vis_d = (float*)(vis_g + w.vcap);
+  r.S.ev_id = nullptr;
+  r.S.hash = (uint32_t*)(base + w.ws);
+  // after the search the hash region holds the prune workspace
+  uint8_t* ws = base + w.ws;
+  const uint32_t cb = r16(4ull * w.ccap);
+  r.Pm = prune_ws((uint32_t*)ws, (float*)(ws + cb), ws + 2 * cb, w.ccap);
+  return r;
+}
+
+// query / debug layout: everything in shared memory
+__device__ __forceinline__ WarpPtrs carve_query(uint8_t* base, const WarpLayout& w) {
   WarpPtrs r;
   r.S.qv = base + w.qv;
   r.S.fr_id = (uint32_t*)(base + w.fr_id);
@@ -69,17 +103,9 @@ __device__ __forceinline__ WarpPtrs carve(uint8_t* base, const WarpLayout& w) {
   r.S.s_d = (float*)(base + w.s_d);
   r.S.vis_id = (uint32_t*)(base + w.vis_id);
   r.S.vis_d = (float*)(base + w.vis_d);
-  r.S.hash = (uint32_t*)(base + w.ws);
-  r.S.ev_id = (uint32_t*)(base + w.ws + (4u << w.hbits));
-  // prune workspace overlays the hash region (dead after the search)
-  r.Pm.cid = r.S.vis_id;
-  r.Pm.ckey = r.S.vis_d;
-  uint8_t* ws = base + w.ws;
-  uint32_t lb = r16(4ull * w.ccap);
-  r.Pm.leaf_lo = (int*)ws;
-  r.Pm.leaf_hi = (int*)(ws + lb);
-  r.Pm.stack = (int*)(ws + 2 * lb);
-  r.Pm.scalar = (int*)(ws + 2 * lb + r16(4ull * ddsort::stack_ints((int)w.ccap)));
+  r.S.ev_id = (uint32_t*)(base + w.ws);
+  r.S.hash = (uint32_t*)(base + w.ws + r16(4ull * w.vcap));
+  r.Pm = PruneSmem{};
   return r;
 }
 
@@ -102,27 +128,35 @@ __device__ __forceinline__ uint32_t row_degree(const uint32_t* row, uint32_t Rp)
 }
 
 // ============================================================ build round
-template <int DT, int MT>
-__global__ void __launch_bounds__(128) k_search_prune(IndexView ix, RoundArgs ra, WarpLayout lay) {
+template <int DT, int MT, int FPL, int CPL>
+__global__ void __launch_bounds__(64, 6) k_search_prune(IndexView ix, RoundArgs ra, WarpLayout lay) {
   extern __shared__ uint4 smem_raw[];
   const uint32_t wpc = blockDim.x >> 5;
   const uint32_t wic = threadIdx.x >> 5;
   const uint32_t lane = lane_id();
-  WarpPtrs W = carve((uint8_t*)smem_raw + (size_t)wic * lay.total, lay);
+  const uint64_t gw = (uint64_t)blockIdx.x * wpc + wic;
+  WarpPtrs W = carve_build((uint8_t*)smem_raw + (size_t)wic * lay.total, lay,
+                           ra.vis_arena + gw * 2ull * lay.vcap);
   SearchParams P;
   P.points = ix.points; P.stride = ix.stride; P.graph = ix.graph; P.Rp = ix.Rp; P.n = ix.n;
   P.d = ix.d; P.start = ra.start; P.L = ra.L; P.k = 0; P.cut = 0.0; P.limit = ix.n;
   P.degree_limit = ix.R; P.hbits = lay.hbits; P.vcap = lay.vcap; P.query_mode = 0;
   P.keep_visited = 1; P.err = ix.err;
   const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
-  for (uint64_t b = (uint64_t)blockIdx.x * wpc + wic; b < ra.B; b += (uint64_t)gridDim.x * wpc) {
+  for (uint64_t b = gw; b < ra.B; b += (uint64_t)gridDim.x * wpc) {
     const uint32_t p = (uint32_t)(ra.floor + b);
     load_vec(W.S.qv, ix.points + (uint64_t)p * ix.stride, qb);
     __syncwarp();
-    SearchOut o = warp_beam_search<DT, MT>(P, W.S, p);
+    SearchOut o = warp_beam_search<DT, MT, FPL, CPL>(P, W.S, p);
     uint32_t m = o.vis_n;
-    // the reference's visited list is sorted by (dist, id)
-    warp_sort_pairs(W.S.vis_id, W.S.vis_d, m);
+    // the visited list moves into the (now free) hash region, sorted by
+    // (dist, id) like the reference's
+    for (uint32_t j = lane; j < m; j += 32) {
+      W.Pm.cid[j] = W.S.vis_id[j];
+      W.Pm.ckey[j] = W.S.vis_d[j];
+    }
+    __syncwarp();
+    warp_sort_pairs(W.Pm.cid, W.Pm.ckey, m);
     // robustPrune adds p's current out-list (round-start snapshot)
     const uint32_t* prow = ix.graph + (uint64_t)p * ix.Rp;
     for (uint32_t base = 0; base < ix.Rp; base += 32) {
@@ -159,127 +193,38 @@ __global__ void k_apply_rows(uint32_t* graph, const uint32_t* new_out, uint64_t 
     dst[i] = src[i];
 }
 
-__global__ void k_emit_count(const uint32_t* new_out, uint64_t total, uint32_t* cnt,
-                             uint32_t* touched, uint32_t* counters) {
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t t = new_out[i];
-    if (t == DD_NONE) continue;
-    if (atomicAdd(&cnt[t], 1u) == 0u) touched[atomicAdd(&counters[0], 1u)] = t;
-  }
-}
-
-// ---- exclusive scan of cnt[touched[i]] over the touched list (length in counters[0])
-__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total, uint32_t* sh) {
-  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  uint32_t x = v;
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= (uint32_t)o) x += y;
-  }
-  if (lane == 31) sh[w] = x;
-  __syncthreads();
-  if (w == 0) {
-    uint32_t s = lane < nw ? sh[lane] : 0;
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
-      if (lane >= (uint32_t)o) s += y;
-    }
-    if (lane < nw) sh[lane] = s;
-  }
-  __syncthreads();
-  uint32_t wbase = w ? sh[w - 1] : 0;
-  *total = sh[nw - 1];
-  __syncthreads();
-  return wbase + x - v;
-}
-
-__global__ void k_scan1(const uint32_t* touched, const uint32_t* cnt, const uint32_t* counters,
-                        uint32_t* block_sums) {
-  uint32_t T = counters[0];
-  uint32_t chunk = (T + gridDim.x - 1) / gridDim.x;
-  uint32_t lo = blockIdx.x * chunk, hi = min(T, lo + chunk);
-  uint32_t s = 0;
-  for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) s += cnt[touched[i]];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  __shared__ uint32_t sh[32];
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t t = 0;
-    for (uint32_t w = 0; w < (blockDim.x >> 5); w++) t += sh[w];
-    block_sums[blockIdx.x] = t;
-  }
-}
-
-__global__ void k_scan2(uint32_t* block_sums, int nb) {
-  __shared__ uint32_t sh[32];
-  uint32_t v = threadIdx.x < (uint32_t)nb ? block_sums[threadIdx.x] : 0;
-  uint32_t tot;
-  uint32_t ex = block_exclusive_scan(v, &tot, sh);
-  if (threadIdx.x < (uint32_t)nb) block_sums[threadIdx.x] = ex;
-}
-
-__global__ void k_scan3(const uint32_t* touched, const uint32_t* cnt, const uint32_t* counters,
-                        const uint32_t* block_sums, uint32_t* seg_start, uint32_t* cursor) {
-  __shared__ uint32_t sh[32];
-  uint32_t T = counters[0];
-  uint32_t chunk = (T + gridDim.x - 1) / gridDim.x;
-  uint32_t lo = blockIdx.x * chunk, hi = min(T, lo + chunk);
-  uint32_t run = block_sums[blockIdx.x];
-  for (uint32_t base = lo; base < hi; base += blockDim.x) {
-    uint32_t i = base + threadIdx.x;
-    uint32_t t = i < hi ? touched[i] : 0;
-    uint32_t v = i < hi ? cnt[t] : 0;
-    uint32_t tot;
-    uint32_t ex = block_exclusive_scan(v, &tot, sh);
-    if (i < hi) {
-      seg_start[i] = run + ex;
-      cursor[t] = run + ex;
-    }
-    run += tot;
-  }
-}
-
-__global__ void k_scatter(const uint32_t* new_out, uint64_t total, uint32_t* cursor,
-                          uint32_t* keys) {
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t t = new_out[i];
-    if (t == DD_NONE) continue;
-    keys[atomicAdd(&cursor[t], 1u)] = (uint32_t)i;  // i = b*Rp + j: batch order
-  }
-}
-
 // per-warp shared layout of the reverse kernel
 struct RevLayout {
-  uint32_t tv, keys, cid, ckey, lo, hi, stack, scalar, total;
+  uint32_t tv, cid, ckey, ws, total;
 };
 __host__ __device__ inline RevLayout rev_layout(uint32_t d, int dtype) {
   RevLayout r;
   uint32_t off = 0;
   uint32_t esz = dtype == DD_F32 ? 4 : 1;
-  auto a16 = [](uint64_t x) { return (uint32_t)((x + 15) & ~(uint64_t)15); };
-  r.tv = off; off += a16((uint64_t)d * esz);
-  r.keys = off; off += a16(4ull * kRevCandCap);
-  r.cid = off; off += a16(4ull * kRevCandCap);
-  r.ckey = off; off += a16(4ull * kRevCandCap);
-  r.lo = off; off += a16(4ull * kRevCandCap);
-  r.hi = off; off += a16(4ull * kRevCandCap);
-  r.stack = off; off += a16(4ull * ddsort::stack_ints((int)kRevCandCap));
-  r.scalar = off; off += 16;
+  r.tv = off; off += r16((uint64_t)d * esz);
+  r.cid = off; off += r16(4ull * kRevCandCap);
+  r.ckey = off; off += r16(4ull * kRevCandCap);
+  r.ws = off; off += prune_ws_bytes(kRevCandCap);
   r.total = off;
   return r;
 }
 
-// Append the (sorted) sources, or prune when the row would exceed R.
-// `sk` holds the s segment keys sorted ascending.
+// The segment of sorted pairs for one target: [start, end) of rs.st / rs.sv.
+__device__ __forceinline__ void segment_of(const ReverseScratch& rs, uint32_t k, uint32_t& start,
+                                           uint32_t& end) {
+  start = rs.heads[k];
+  end = (k + 1 < rs.counters[1]) ? rs.heads[k + 1] : rs.counters[0];
+}
+
+// Append the sources of segment [start, end) (already in batch order), or
+// prune when the row would exceed R (one warp; s + deg <= kRevCandCap).
 template <int DT, int MT>
-__device__ void reverse_one(const IndexView& ix, const RoundArgs& ra, uint32_t t, uint32_t s,
-                            const uint32_t* sk, uint32_t deg, uint8_t* tv, PruneSmem Pm,
-                            uint32_t* counters) {
+__device__ void reverse_one(const IndexView& ix, const RoundArgs& ra, const ReverseScratch& rs,
+                            uint32_t t, uint32_t start, uint32_t s, uint32_t deg, uint8_t* tv,
+                            PruneSmem Pm) {
   const uint32_t lane = lane_id();
   uint32_t* row = ix.graph + (uint64_t)t * ix.Rp;
+  const uint32_t* sk = rs.sv + start;
   if (s + deg <= ix.R) {
     for (uint32_t j = lane; j < s; j += 32) row[deg + j] = (uint32_t)(ra.floor + sk[j] / ix.Rp);
     __syncwarp();
@@ -303,8 +248,8 @@ __device__ void reverse_one(const IndexView& ix, const RoundArgs& ra, uint32_t t
   warp_std_sort(Pm, m);
   warp_greedy_select<DT, MT>(ix.points, ix.stride, ix.d, t, Pm, m, ra.alpha, ix.R, row, ix.Rp);
   if (lane == 0) {
-    atomicAdd(&counters[2], 1u);
-    atomicAdd(&counters[3], m);
+    atomicAdd(&rs.counters[2], 1u);
+    atomicAdd(&rs.counters[3], m);
   }
 }
 
@@ -314,83 +259,211 @@ __global__ void __launch_bounds__(kRevWarps * 32) k_reverse(IndexView ix, RoundA
   const RevLayout L = rev_layout(ix.d, DT);
   const uint32_t wic = threadIdx.x >> 5, lane = lane_id();
   uint8_t* base = (uint8_t*)smem_raw + (size_t)wic * L.total;
-  uint32_t* sk = (uint32_t*)(base + L.keys);
-  PruneSmem Pm{(uint32_t*)(base + L.cid), (float*)(base + L.ckey), (int*)(base + L.lo),
-               (int*)(base + L.hi), (int*)(base + L.stack), (int*)(base + L.scalar)};
-  const uint32_t T = rs.counters[0];
-  for (uint32_t i = blockIdx.x * kRevWarps + wic; i < T; i += gridDim.x * kRevWarps) {
-    const uint32_t t = rs.touched[i];
-    const uint32_t s = rs.cnt[t];
-    const uint32_t st0 = rs.seg_start[i];
+  PruneSmem Pm = prune_ws((uint32_t*)(base + L.cid), (float*)(base + L.ckey), base + L.ws,
+                          kRevCandCap);
+  const uint32_t T = rs.counters[1];
+  for (uint32_t k = blockIdx.x * kRevWarps + wic; k < T; k += gridDim.x * kRevWarps) {
+    uint32_t start, end;
+    segment_of(rs, k, start, end);
+    const uint32_t t = rs.st[start];
+    const uint32_t s = end - start;
     const uint32_t deg = row_degree(ix.graph + (uint64_t)t * ix.Rp, ix.Rp);
     if (s + deg > kRevCandCap) {
-      if (lane == 0) rs.big[atomicAdd(&rs.counters[1], 1u)] = i;
-      continue;  // handled by k_reverse_big (which also clears cnt[t])
+      if (lane == 0) {
+        atomicMax(&rs.counters[5], s + deg);  // largest candidate list of the round
+        rs.big[atomicAdd(&rs.counters[4], 1u)] = k;
+      }
+      continue;  // handled by k_reverse_big
     }
-    for (uint32_t j = lane; j < s; j += 32) sk[j] = rs.keys[st0 + j];
-    __syncwarp();
-    warp_sort_u32(sk, s);
-    reverse_one<DT, MT>(ix, ra, t, s, sk, deg, base + L.tv, Pm, rs.counters);
-    if (lane == 0) rs.cnt[t] = 0;
-    __syncwarp();
+    reverse_one<DT, MT>(ix, ra, rs, t, start, s, deg, base + L.tv, Pm);
   }
 }
 
-// Large targets: same logic with the candidate workspace in global memory.
-// One warp per entry; `slot` selects this warp's workspace slice.
+// Targets with more than kRevCandCap candidates: one CTA each, candidates in
+// this CTA's global workspace slice.  The sort emulation splits the work:
+// ranges longer than kCtaRange are partitioned by the whole CTA, shorter ones
+// by single warps; then all threads finish the leaves.  The greedy selection
+// spreads each occlusion pass over the CTA and compacts the survivors while
+// the list is long.
+constexpr int kCtaRange = 4096;
+constexpr int kBigStackInts = 3 * 72;
+
 template <int DT, int MT>
-__global__ void k_reverse_big(IndexView ix, RoundArgs ra, ReverseScratch rs) {
-  __shared__ __align__(16) uint8_t tvbuf[4 * 1024];
-  __shared__ int scalar[4];
-  const uint32_t lane = lane_id();
-  const uint32_t slot = blockIdx.x;
-  uint32_t* cid = rs.gcand + (uint64_t)slot * rs.gcap;
-  float* ckey = rs.gkey + (uint64_t)slot * rs.gcap;
-  int* lo = rs.gleaf + (uint64_t)slot * (2 * rs.gcap + ddsort::stack_ints((int)rs.gcap));
-  int* hi = lo + rs.gcap;
-  int* stack = hi + rs.gcap;
-  PruneSmem Pm{cid, ckey, lo, hi, stack, scalar};
-  const uint32_t nbig = rs.counters[1];
-  for (uint32_t e = slot; e < nbig; e += gridDim.x) {
-    const uint32_t i = rs.big[e];
-    const uint32_t t = rs.touched[i];
-    const uint32_t s = rs.cnt[t];
-    const uint32_t st0 = rs.seg_start[i];
-    const uint32_t deg = row_degree(ix.graph + (uint64_t)t * ix.Rp, ix.Rp);
-    if ((uint64_t)s + deg > rs.gcap) {
-      if (lane == 0) dd_set_error(ix.err, DD_ESEG_CAP);
+__global__ void __launch_bounds__(kBigThreads) k_reverse_big(IndexView ix, RoundArgs ra, ReverseScratch rs) {
+  __shared__ __align__(16) uint8_t tv[1024];
+  __shared__ uint32_t sh[32];
+  __shared__ int cstack[kBigStackInts];
+  __shared__ int wstack[kBigThreads / 32][kBigStackInts];
+  __shared__ uint32_t s_deg, s_nsmall, s_next, s_mm;
+  const uint32_t tid = threadIdx.x, lane = lane_id(), wid = tid >> 5;
+  const uint64_t cap = rs.gcap;
+  const uint64_t slot = blockIdx.x;
+  uint32_t* cid = rs.gcand + slot * cap;
+  float* ckey = rs.gkey + slot * cap;
+  int* posL = rs.gpos + slot * 2 * cap;
+  int* posR = posL + cap;
+  uint32_t* bits = rs.gbits + slot * (cap / 32 + 2);
+  int* ranges = rs.granges + slot * 3 * (cap / 8 + 64);
+  const uint32_t nbig = rs.counters[4];
+  ddsort::Arr<uint32_t> A{cid, ckey};
+  for (uint32_t e = blockIdx.x; e < nbig; e += gridDim.x) {
+    const uint32_t k = rs.big[e];
+    uint32_t start, end;
+    segment_of(rs, k, start, end);
+    const uint32_t t = rs.st[start];
+    const uint32_t s = end - start;
+    uint32_t* row = ix.graph + (uint64_t)t * ix.Rp;
+    if (wid == 0) {
+      uint32_t dg = row_degree(row, ix.Rp);
+      if (lane == 0) s_deg = dg;
+    }
+    const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
+    for (uint32_t j = tid; j < qb / 16; j += blockDim.x)
+      ((uint4*)tv)[j] = __ldg((const uint4*)(ix.points + (uint64_t)t * ix.stride) + j);
+    __syncthreads();
+    const uint32_t deg = s_deg;
+    const uint32_t m = s + deg;
+    if ((uint64_t)m > cap) {  // cannot happen: s <= batch size, cap = batch + Rp
+      if (tid == 0) dd_set_error(ix.err, DD_ESEG_CAP);
+      __syncthreads();
       continue;
     }
-    // the segment keys are sorted in place in the key buffer
-    uint32_t* sk = rs.keys + st0;
-    warp_sort_u32(sk, s);
-    reverse_one<DT, MT>(ix, ra, t, s, sk, deg, tvbuf, Pm, rs.counters);
-    if (lane == 0) rs.cnt[t] = 0;
-    __syncwarp();
+    for (uint32_t j = tid; j < s; j += blockDim.x) {
+      uint32_t c = (uint32_t)(ra.floor + rs.sv[start + j] / ix.Rp);
+      cid[j] = c;
+      ckey[j] = Dist<DT, MT>::eval(tv, ix.points + (uint64_t)c * ix.stride, ix.d);
+    }
+    for (uint32_t j = tid; j < deg; j += blockDim.x) {
+      uint32_t c = row[j];
+      cid[s + j] = c;
+      ckey[s + j] = Dist<DT, MT>::eval(tv, ix.points + (uint64_t)c * ix.stride, ix.d);
+    }
+    for (uint32_t w = tid; w < (m + 31) / 32; w += blockDim.x) bits[w] = 0;
+    if (tid == 0) {
+      s_nsmall = 0;
+      s_next = 0;
+      cstack[0] = 0;
+      cstack[1] = (int)m;
+      cstack[2] = 2 * ddsort::floor_log2((int)m);
+    }
+    __syncthreads();
+    // ---- sort emulation, phase 1: long ranges, whole CTA
+    int sp = 3;
+    while (sp > 0) {
+      int depth = cstack[sp - 1], last = cstack[sp - 2], first = cstack[sp - 3];
+      sp -= 3;
+      __syncthreads();
+      while (last - first > kCtaRange && depth > 0) {
+        --depth;
+        const int mid = first + (last - first) / 2;
+        if (tid == 0) ddsort::move_median_to_first(A, first, first + 1, mid, last - 1);
+        __syncthreads();
+        const int cut = cta_partition_rank(A, first + 1, last, first, posL, posR, sh);
+        if (tid == 0) {
+          cstack[sp] = cut;
+          cstack[sp + 1] = last;
+          cstack[sp + 2] = depth;
+        }
+        sp += 3;
+        last = cut;
+        __syncthreads();
+      }
+      if (tid == 0) {  // the rest of this range goes to a warp
+        int r = (int)s_nsmall++;
+        ranges[3 * r] = first;
+        ranges[3 * r + 1] = last;
+        ranges[3 * r + 2] = depth;
+      }
+      __syncthreads();
+    }
+    // ---- phase 2: short ranges, one warp each (disjoint scratch: posL + first)
+    while (true) {
+      uint32_t r = 0;
+      if (lane == 0) r = atomicAdd(&s_next, 1u);
+      r = __shfl_sync(0xffffffffu, r, 0);
+      if (r >= s_nsmall) break;
+      const int first = ranges[3 * r], last = ranges[3 * r + 1], depth = ranges[3 * r + 2];
+      warp_partition_loop(A, first, last, depth, wstack[wid], bits, posL + first, posR + first,
+                          true);
+    }
+    __syncthreads();
+    // ---- phase 3: leaves
+    for (uint32_t q = tid; q < m; q += blockDim.x)
+      if (bits[q >> 5] & (1u << (q & 31)))
+        ddsort::insertion_sort_range(A, (int)q, ddsort::leaf_end(bits, (int)q, (int)m));
+    __syncthreads();
+    // ---- greedy selection (the row of t is rewritten; its old entries are in cid)
+    uint32_t nsel = 0, idx = 0, mm = m;
+    while (nsel < ix.R && idx < mm) {
+      const uint32_t ps = cid[idx];
+      idx++;
+      if (ps == t || ps == DD_NONE) continue;
+      if (tid == 0) row[nsel] = ps;
+      nsel++;
+      const uint8_t* prow = ix.points + (uint64_t)ps * ix.stride;
+      for (uint32_t q = idx + tid; q < mm; q += blockDim.x) {
+        const uint32_t c = cid[q];
+        if (c != DD_NONE) {
+          const float dsp = Dist<DT, MT>::eval(prow, ix.points + (uint64_t)c * ix.stride, ix.d);
+          if (__dmul_rn(ra.alpha, (double)dsp) <= (double)ckey[q]) cid[q] = DD_NONE;
+        }
+      }
+      __syncthreads();
+      if (mm - idx > 2048) {  // compact [idx, mm): drop removed entries, keep the order
+        const uint32_t n2 = mm - idx;
+        const uint32_t ch = (n2 + blockDim.x - 1) / blockDim.x;
+        const uint32_t lo = idx + tid * ch, hi = min(mm, lo + ch);
+        uint32_t c = 0;
+        for (uint32_t q = lo; q < hi; q++) c += cid[q] != DD_NONE ? 1u : 0u;
+        uint32_t tot;
+        uint32_t w = cta_scan_excl(c, &tot, sh);
+        for (uint32_t q = lo; q < hi; q++)
+          if (cid[q] != DD_NONE) {
+            posL[w] = (int)cid[q];
+            posR[w] = __float_as_int(ckey[q]);
+            w++;
+          }
+        __syncthreads();
+        for (uint32_t q = tid; q < tot; q += blockDim.x) {
+          cid[idx + q] = (uint32_t)posL[q];
+          ckey[idx + q] = __int_as_float(posR[q]);
+        }
+        if (tid == 0) s_mm = idx + tot;
+        __syncthreads();
+        mm = s_mm;
+      }
+    }
+    for (uint32_t j = nsel + tid; j < ix.Rp; j += blockDim.x) row[j] = DD_NONE;
+    if (tid == 0) {
+      atomicAdd(&rs.counters[2], 1u);
+      atomicAdd(&rs.counters[3], m);
+    }
+    __syncthreads();
   }
 }
 
 // ============================================================ queries
-template <int DT, int MT>
+template <int DT, int MT, int FPL, int CPL>
 __global__ void __launch_bounds__(128) k_query(IndexView ix, QueryArgs qa, WarpLayout lay) {
   extern __shared__ uint4 smem_raw[];
   const uint32_t wpc = blockDim.x >> 5, wic = threadIdx.x >> 5, lane = lane_id();
-  WarpPtrs W = carve((uint8_t*)smem_raw + (size_t)wic * lay.total, lay);
+  const uint64_t gw = (uint64_t)blockIdx.x * wpc + wic;
+  WarpPtrs W = carve_query((uint8_t*)smem_raw + (size_t)wic * lay.total, lay);
   const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
-  for (uint64_t q = (uint64_t)blockIdx.x * wpc + wic; q < qa.nq; q += (uint64_t)gridDim.x * wpc) {
+  for (uint64_t q = gw; q < qa.nq; q += (uint64_t)gridDim.x * wpc) {
     SearchParams P;
-    P.points = ix.points; P.stride = ix.stride; P.graph = ix.graph; P.Rp = ix.Rp; P.n = ix.n;
     uint32_t Lq = qa.Ls[q];
     if (Lq == 0 || Lq > qa.Lmax || Lq < qa.k) {
       if (lane == 0) dd_set_error(ix.err, DD_ECAND_CAP);
       Lq = qa.Lmax;
     }
+    P.points = ix.points; P.stride = ix.stride; P.graph = ix.graph; P.Rp = ix.Rp; P.n = ix.n;
     P.d = ix.d; P.start = qa.start; P.L = Lq; P.k = qa.k; P.cut = qa.cut; P.limit = qa.limit;
     P.degree_limit = qa.degree_limit; P.hbits = hash_bits_for(P.L); P.vcap = lay.vcap;
     P.query_mode = 1; P.keep_visited = 0; P.err = ix.err;
     load_vec(W.S.qv, qa.queries + q * qa.qstride, qb);
     __syncwarp();
-    SearchOut o = warp_beam_search<DT, MT>(P, W.S, qa.skip_self ? q : (uint64_t)-1);
+    SearchOut o = warp_beam_search<DT, MT, FPL, CPL>(P, W.S, qa.skip_self ? q : (uint64_t)-1);
     for (uint32_t j = lane; j < qa.k; j += 32) {
       bool v = j < o.fr_n;
       qa.ids[q * qa.k + j] = v ? (W.S.fr_id[j] & ~DD_VBIT) : DD_NONE;
@@ -408,7 +481,7 @@ template <int DT, int MT>
 __global__ void __launch_bounds__(32) k_beam(IndexView ix, BeamArgs ba, WarpLayout lay) {
   extern __shared__ uint4 smem_raw[];
   const uint32_t lane = lane_id();
-  WarpPtrs W = carve((uint8_t*)smem_raw, lay);
+  WarpPtrs W = carve_query((uint8_t*)smem_raw, lay);
   const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
   for (uint64_t q = blockIdx.x; q < ba.nq; q += gridDim.x) {
     SearchParams P;
@@ -418,7 +491,7 @@ __global__ void __launch_bounds__(32) k_beam(IndexView ix, BeamArgs ba, WarpLayo
     P.query_mode = ba.k > 0; P.keep_visited = 1; P.err = ix.err;
     load_vec(W.S.qv, ba.queries + q * ba.qstride, qb);
     __syncwarp();
-    SearchOut o = warp_beam_search<DT, MT>(P, W.S, (uint64_t)ba.self_ids[q]);
+    SearchOut o = warp_beam_search<DT, MT, 16, 4>(P, W.S, (uint64_t)ba.self_ids[q]);
     warp_sort_pairs(W.S.vis_id, W.S.vis_d, o.vis_n);
     for (uint32_t j = lane; j < o.fr_n; j += 32) {
       ba.fr_ids[q * ba.L + j] = W.S.fr_id[j] & ~DD_VBIT;
@@ -440,7 +513,6 @@ __global__ void __launch_bounds__(32) k_beam(IndexView ix, BeamArgs ba, WarpLayo
 // robustPrune on explicit candidate lists: one warp per task, global workspace
 template <int DT, int MT>
 __global__ void k_prune_tasks(IndexView ix, PruneArgs pa) {
-  __shared__ int scalar[4];
   const uint32_t lane = lane_id();
   for (uint32_t t = blockIdx.x; t < pa.ntasks; t += gridDim.x) {
     const uint32_t p = pa.p[t];
@@ -449,9 +521,7 @@ __global__ void k_prune_tasks(IndexView ix, PruneArgs pa) {
     const uint64_t cap = (o1 - o0) + ix.Rp;
     uint32_t* cid = pa.gcand + wbase;
     float* ckey = pa.gkey + wbase;
-    int* lo = pa.gleaf + 2 * wbase + (uint64_t)t * kGlobalStackInts;
-    int* hi = lo + cap;
-    int* stack = hi + cap;
+    uint8_t* ws = (uint8_t*)(pa.gws + 3 * wbase + (uint64_t)t * kGlobalStackInts);
     uint32_t m = (uint32_t)(o1 - o0);
     for (uint32_t j = lane; j < m; j += 32) {
       cid[j] = pa.cand_ids[o0 + j];
@@ -472,7 +542,7 @@ __global__ void k_prune_tasks(IndexView ix, PruneArgs pa) {
       m += __popc(vb);
     }
     __syncwarp();
-    PruneSmem Pm{cid, ckey, lo, hi, stack, scalar};
+    PruneSmem Pm = prune_ws(cid, ckey, ws, (uint32_t)cap);
     warp_std_sort(Pm, m);
     warp_greedy_select<DT, MT>(ix.points, ix.stride, ix.d, p, Pm, m, pa.alpha, ix.R,
                                pa.out + (uint64_t)t * ix.Rp, ix.Rp);
@@ -485,10 +555,9 @@ template <int DT, int MT>
 __global__ void __launch_bounds__(32) k_sort_rows(IndexView ix) {
   __shared__ uint32_t cid[kMaxRp];
   __shared__ float ckey[kMaxRp];
-  __shared__ int lo[kMaxRp], hi[kMaxRp];
-  __shared__ int stack[64];
-  __shared__ int scalar[4];
+  __shared__ __align__(16) uint8_t ws[2048];  // >= prune_ws_bytes(kMaxRp)
   const uint32_t lane = lane_id();
+  PruneSmem Pm = prune_ws(cid, ckey, ws, kMaxRp);
   for (uint64_t v = blockIdx.x; v < ix.n; v += gridDim.x) {
     uint32_t* row = ix.graph + v * ix.Rp;
     const uint8_t* pv = ix.points + v * ix.stride;
@@ -498,7 +567,6 @@ __global__ void __launch_bounds__(32) k_sort_rows(IndexView ix) {
       ckey[j] = Dist<DT, MT>::eval(pv, ix.points + (uint64_t)row[j] * ix.stride, ix.d);
     }
     __syncwarp();
-    PruneSmem Pm{cid, ckey, lo, hi, stack, scalar};
     warp_std_sort(Pm, deg);
     for (uint32_t j = lane; j < deg; j += 32) row[j] = cid[j];
     __syncwarp();
@@ -526,8 +594,29 @@ __device__ __forceinline__ double exact_dist64(const uint8_t* q, const uint8_t* 
   }
 }
 
-// grid (query blocks of 8 warps, chunks); each warp keeps a top-k (k <= 32)
-// sorted across its lanes by (distance, id)
+// warp-distributed sorted top-k (k <= 32): lane i holds the i-th best (dist, id)
+__device__ __forceinline__ void topk_insert(double& bd, uint32_t& bi, uint32_t k, double dv,
+                                            uint32_t iv, bool cand) {
+  const uint32_t lane = lane_id();
+  uint32_t mask = __ballot_sync(0xffffffffu, cand);
+  while (mask) {
+    int src = __ffs(mask) - 1;
+    mask &= mask - 1;
+    double cd = __shfl_sync(0xffffffffu, dv, src);
+    uint32_t ci = __shfl_sync(0xffffffffu, iv, src);
+    double kd = __shfl_sync(0xffffffffu, bd, k - 1);
+    uint32_t ki = __shfl_sync(0xffffffffu, bi, k - 1);
+    if (!((cd < kd) || (cd == kd && ci < ki))) continue;
+    bool before = (lane < k) && ((bd < cd) || (bd == cd && bi < ci));
+    uint32_t pos = __popc(__ballot_sync(0xffffffffu, before));
+    double ud = __shfl_up_sync(0xffffffffu, bd, 1);
+    uint32_t ui = __shfl_up_sync(0xffffffffu, bi, 1);
+    if (lane == pos) { bd = cd; bi = ci; }
+    else if (lane > pos) { bd = ud; bi = ui; }
+  }
+}
+
+// grid (query blocks of 8 warps, chunks); each warp keeps a top-k of its chunk
 template <int DT, int MT>
 __global__ void __launch_bounds__(256) k_gt_partial(IndexView ix, const uint8_t* queries, uint64_t qstride,
                                                     uint64_t nq, uint32_t k, uint32_t nchunks,
@@ -554,23 +643,7 @@ __global__ void __launch_bounds__(256) k_gt_partial(IndexView ix, const uint8_t*
     }
     double td = __shfl_sync(0xffffffffu, bd, k - 1);
     uint32_t ti = __shfl_sync(0xffffffffu, bi, k - 1);
-    bool cand = (dv < td) || (dv == td && iv < ti);
-    uint32_t mask = __ballot_sync(0xffffffffu, cand);
-    while (mask) {
-      int src = __ffs(mask) - 1;
-      mask &= mask - 1;
-      double cd = __shfl_sync(0xffffffffu, dv, src);
-      uint32_t ci = __shfl_sync(0xffffffffu, iv, src);
-      double kd = __shfl_sync(0xffffffffu, bd, k - 1);
-      uint32_t ki = __shfl_sync(0xffffffffu, bi, k - 1);
-      if (!((cd < kd) || (cd == kd && ci < ki))) continue;
-      bool before = (lane < k) && ((bd < cd) || (bd == cd && bi < ci));
-      uint32_t pos = __popc(__ballot_sync(0xffffffffu, before));
-      double ud = __shfl_up_sync(0xffffffffu, bd, 1);
-      uint32_t ui = __shfl_up_sync(0xffffffffu, bi, 1);
-      if (lane == pos) { bd = cd; bi = ci; }
-      else if (lane > pos) { bd = ud; bi = ui; }
-    }
+    topk_insert(bd, bi, k, dv, iv, (dv < td) || (dv == td && iv < ti));
   }
   if (lane < k) {
     uint64_t o = (q * nchunks + blockIdx.y) * k + lane;
@@ -593,23 +666,7 @@ __global__ void k_gt_merge(const double* part_d, const uint32_t* part_i, uint64_
     uint32_t iv = e < tot ? part_i[q * tot + e] : DD_NONE;
     double td = __shfl_sync(0xffffffffu, bd, k - 1);
     uint32_t ti = __shfl_sync(0xffffffffu, bi, k - 1);
-    bool cand = (dv < td) || (dv == td && iv < ti);
-    uint32_t mask = __ballot_sync(0xffffffffu, cand);
-    while (mask) {
-      int src = __ffs(mask) - 1;
-      mask &= mask - 1;
-      double cd = __shfl_sync(0xffffffffu, dv, src);
-      uint32_t ci = __shfl_sync(0xffffffffu, iv, src);
-      double kd = __shfl_sync(0xffffffffu, bd, k - 1);
-      uint32_t ki = __shfl_sync(0xffffffffu, bi, k - 1);
-      if (!((cd < kd) || (cd == kd && ci < ki))) continue;
-      bool before = (lane < k) && ((bd < cd) || (bd == cd && bi < ci));
-      uint32_t pos = __popc(__ballot_sync(0xffffffffu, before));
-      double ud = __shfl_up_sync(0xffffffffu, bd, 1);
-      uint32_t ui = __shfl_up_sync(0xffffffffu, bi, 1);
-      if (lane == pos) { bd = cd; bi = ci; }
-      else if (lane > pos) { bd = ud; bi = ui; }
-    }
+    topk_insert(bd, bi, k, dv, iv, (dv < td) || (dv == td && iv < ti));
   }
   if (lane < k) {
     ids[q * k + lane] = bi;
@@ -659,14 +716,23 @@ __global__ void k_from_ref_rows(uint32_t* graph, uint64_t n, uint32_t R, uint32_
 }
 
 // ============================================================ launchers
-#define DD_DISPATCH(dtype, metric, KERNEL_CALL)                      \
-  do {                                                               \
-    if ((dtype) == DD_F32 && (metric) == DD_L2) { KERNEL_CALL(DD_F32, DD_L2); }        \
-    else if ((dtype) == DD_F32) { KERNEL_CALL(DD_F32, DD_MIPS); }                      \
-    else if ((dtype) == DD_I8 && (metric) == DD_L2) { KERNEL_CALL(DD_I8, DD_L2); }     \
-    else if ((dtype) == DD_I8) { KERNEL_CALL(DD_I8, DD_MIPS); }                        \
-    else if ((metric) == DD_L2) { KERNEL_CALL(DD_U8, DD_L2); }                         \
-    else { KERNEL_CALL(DD_U8, DD_MIPS); }                                              \
+#define DD_DISPATCH_DM(dtype, metric, CALL)                                          \
+  do {                                                                               \
+    if ((dtype) == DD_F32 && (metric) == DD_L2) { CALL(DD_F32, DD_L2); }             \
+    else if ((dtype) == DD_F32) { CALL(DD_F32, DD_MIPS); }                           \
+    else if ((dtype) == DD_I8 && (metric) == DD_L2) { CALL(DD_I8, DD_L2); }          \
+    else if ((dtype) == DD_I8) { CALL(DD_I8, DD_MIPS); }                             \
+    else if ((metric) == DD_L2) { CALL(DD_U8, DD_L2); }                              \
+    else { CALL(DD_U8, DD_MIPS); }                                                   \
+  } while (0)
+
+// frontier / row register buckets: (L <= 128 | L <= 512) x (Rp <= 64 | Rp <= 128)
+#define DD_DISPATCH_FC(L, Rp, DT, MT, CALL4)                                         \
+  do {                                                                               \
+    if ((L) <= 128 && (Rp) <= 64) { CALL4(DT, MT, 4, 2); }                           \
+    else if ((L) <= 128) { CALL4(DT, MT, 4, 4); }                                    \
+    else if ((Rp) <= 64) { CALL4(DT, MT, 16, 2); }                                   \
+    else { CALL4(DT, MT, 16, 4); }                                                   \
   } while (0)
 
 template <typename K>
@@ -674,14 +740,37 @@ static void set_smem(K kernel, size_t bytes) {
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+template <typename K>
+static int occupancy(K kernel, int threads, size_t smem) {
+  set_smem(kernel, smem);
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, smem) != cudaSuccess) b = 1;
+  return b > 0 ? b : 1;
+}
+
+int search_blocks_per_sm(const IndexView& ix, const WarpLayout& lay, uint32_t L, int wpc, bool build) {
+  size_t sm = (size_t)lay.total * wpc;
+  int b = 1;
+#define OCC4(DT, MT, F, C)                                                            \
+  b = build ? occupancy(k_search_prune<DT, MT, F, C>, wpc * 32, sm)                   \
+            : occupancy(k_query<DT, MT, F, C>, wpc * 32, sm);
+#define OCC(DT, MT) DD_DISPATCH_FC(L, ix.Rp, DT, MT, OCC4)
+  DD_DISPATCH_DM(ix.dtype, ix.metric, OCC);
+#undef OCC
+#undef OCC4
+  return b;
+}
+
 void launch_search_prune(const IndexView& ix, const RoundArgs& ra, const WarpLayout& lay,
                          int wpc, int grid, cudaStream_t st) {
   size_t sm = (size_t)lay.total * wpc;
-#define CALL(DT, MT)                                                   \
-  set_smem(k_search_prune<DT, MT>, sm);                                \
-  k_search_prune<DT, MT><<<grid, wpc * 32, sm, st>>>(ix, ra, lay);
-  DD_DISPATCH(ix.dtype, ix.metric, CALL);
+#define CALL4(DT, MT, F, C)                                                          \
+  set_smem(k_search_prune<DT, MT, F, C>, sm);                                        \
+  k_search_prune<DT, MT, F, C><<<grid, wpc * 32, sm, st>>>(ix, ra, lay);
+#define CALL(DT, MT) DD_DISPATCH_FC(ra.L, ix.Rp, DT, MT, CALL4)
+  DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
 #undef CALL
+#undef CALL4
 }
 
 void launch_apply_rows(const IndexView& ix, const RoundArgs& ra, cudaStream_t st) {
@@ -693,51 +782,37 @@ void launch_apply_rows(const IndexView& ix, const RoundArgs& ra, cudaStream_t st
 
 void launch_reverse(const IndexView& ix, const RoundArgs& ra, const ReverseScratch& rs,
                     cudaStream_t st, int sm_count) {
-  uint64_t total = (uint64_t)ra.B * ix.Rp;
-  if (!total) return;
-  int g = (int)std::min<uint64_t>((total + 255) / 256, (uint64_t)sm_count * 16);
-  k_emit_count<<<g, 256, 0, st>>>(ra.new_out, total, rs.cnt, rs.touched, rs.counters);
-  k_scan1<<<kScanBlocks, 256, 0, st>>>(rs.touched, rs.cnt, rs.counters, rs.block_sums);
-  k_scan2<<<1, kScanBlocks, 0, st>>>(rs.block_sums, kScanBlocks);
-  k_scan3<<<kScanBlocks, 256, 0, st>>>(rs.touched, rs.cnt, rs.counters, rs.block_sums,
-                                       rs.seg_start, rs.cursor);
-  k_scatter<<<g, 256, 0, st>>>(ra.new_out, total, rs.cursor, rs.keys);
+  if (!ra.B) return;
   RevLayout L = rev_layout(ix.d, ix.dtype);
   size_t sm = (size_t)L.total * kRevWarps;
   int rg = sm_count * 8;
-#define CALL(DT, MT)                                                    \
-  set_smem(k_reverse<DT, MT>, sm);                                      \
-  k_reverse<DT, MT><<<rg, kRevWarps * 32, sm, st>>>(ix, ra, rs);
-  DD_DISPATCH(ix.dtype, ix.metric, CALL);
-#undef CALL
-}
-
-void launch_reverse_big(const IndexView& ix, const RoundArgs& ra, const ReverseScratch& rs,
-                        uint32_t slots, cudaStream_t st) {
-  // the number of big entries is read on the device; `slots` workspaces exist
-  int g = (int)slots;
-#define CALL(DT, MT) k_reverse_big<DT, MT><<<g, 32, 0, st>>>(ix, ra, rs);
-  DD_DISPATCH(ix.dtype, ix.metric, CALL);
+#define CALL(DT, MT)                                                                  \
+  set_smem(k_reverse<DT, MT>, sm);                                                    \
+  k_reverse<DT, MT><<<rg, kRevWarps * 32, sm, st>>>(ix, ra, rs);                       \
+  k_reverse_big<DT, MT><<<kBigSlots, kBigThreads, 0, st>>>(ix, ra, rs);
+  DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
 #undef CALL
 }
 
 void launch_query(const IndexView& ix, const QueryArgs& qa, const WarpLayout& lay, int wpc,
                   int grid, cudaStream_t st) {
   size_t sm = (size_t)lay.total * wpc;
-#define CALL(DT, MT)                                                   \
-  set_smem(k_query<DT, MT>, sm);                                       \
-  k_query<DT, MT><<<grid, wpc * 32, sm, st>>>(ix, qa, lay);
-  DD_DISPATCH(ix.dtype, ix.metric, CALL);
+#define CALL4(DT, MT, F, C)                                                          \
+  set_smem(k_query<DT, MT, F, C>, sm);                                               \
+  k_query<DT, MT, F, C><<<grid, wpc * 32, sm, st>>>(ix, qa, lay);
+#define CALL(DT, MT) DD_DISPATCH_FC(qa.Lmax, ix.Rp, DT, MT, CALL4)
+  DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
 #undef CALL
+#undef CALL4
 }
 
-void launch_beam(const IndexView& ix, const BeamArgs& ba, const WarpLayout& lay, cudaStream_t st) {
+void launch_beam(const IndexView& ix, const BeamArgs& ba, const WarpLayout& lay, int grid,
+                 cudaStream_t st) {
   size_t sm = lay.total;
-  int grid = (int)std::min<uint64_t>(ba.nq, 4096);
 #define CALL(DT, MT)                                                   \
   set_smem(k_beam<DT, MT>, sm);                                        \
   k_beam<DT, MT><<<grid, 32, sm, st>>>(ix, ba, lay);
-  DD_DISPATCH(ix.dtype, ix.metric, CALL);
+  DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
 #undef CALL
 }
 
@@ -745,14 +820,14 @@ void launch_prune_tasks(const IndexView& ix, const PruneArgs& pa, cudaStream_t s
   if (!pa.ntasks) return;
   int grid = (int)std::min<uint32_t>(pa.ntasks, 4096);
 #define CALL(DT, MT) k_prune_tasks<DT, MT><<<grid, 32, 0, st>>>(ix, pa);
-  DD_DISPATCH(ix.dtype, ix.metric, CALL);
+  DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
 #undef CALL
 }
 
 void launch_sort_rows(const IndexView& ix, cudaStream_t st) {
   int grid = (int)std::min<uint64_t>(ix.n, 65536);
 #define CALL(DT, MT) k_sort_rows<DT, MT><<<grid, 32, 0, st>>>(ix);
-  DD_DISPATCH(ix.dtype, ix.metric, CALL);
+  DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
 #undef CALL
 }
 
@@ -762,7 +837,7 @@ void launch_groundtruth(const IndexView& ix, const uint8_t* queries, uint64_t qs
   dim3 grid((unsigned)((nq + 7) / 8), nchunks);
 #define CALL(DT, MT)                                                                  \
   k_gt_partial<DT, MT><<<grid, 256, 0, st>>>(ix, queries, qstride, nq, k, nchunks, part_d, part_i);
-  DD_DISPATCH(ix.dtype, ix.metric, CALL);
+  DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
 #undef CALL
   k_gt_merge<<<(unsigned)((nq + 7) / 8), 256, 0, st>>>(part_d, part_i, nq, k, nchunks, ids, dists);
 }

@@ -8,14 +8,14 @@ namespace ddk {
 constexpr uint32_t kMaxL = 512;   // frontier capacity: 16 entries per lane
 constexpr uint32_t kMaxRp = 128;  // graph row capacity: 4 candidates per lane
 
-// Per-warp shared-memory carve-up of the fused search+prune kernel and of the
-// query kernel (all offsets in bytes, 16-byte aligned).
+// Per-warp shared-memory carve-up of the search kernels (byte offsets, 16-byte
+// aligned).  The lossy hash table of each search lives in global memory.
 struct WarpLayout {
   uint32_t qv, fr_id, fr_d, c_id, c_d, s_id, s_d, vis_id, vis_d, ws;
   uint32_t total;
-  uint32_t vcap;   // visited/evicted capacity
-  uint32_t ccap;   // prune candidate capacity (vis arrays hold vcap + Rp)
-  uint32_t hbits;
+  uint32_t vcap;   // visited / evicted list capacity
+  uint32_t ccap;   // prune candidate capacity (the visited arrays hold vcap + Rp)
+  uint32_t hbits;  // hash bits of the largest beam width of the launch
 };
 
 struct IndexView {
@@ -31,46 +31,54 @@ struct IndexView {
 
 WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, uint32_t vcap,
                               bool with_prune);
+// warps resident per SM for a layout (occupancy of the search kernels)
+int search_blocks_per_sm(const IndexView& ix, const WarpLayout& lay, uint32_t L, int wpc,
+                         bool build);
 
 struct RoundArgs {
   uint64_t floor;
-  uint32_t B;          // batch points this round
+  uint32_t B;            // batch points this round
   uint32_t L;
   double alpha;
   uint32_t start;
-  uint32_t* new_out;   // B x Rp
-  uint32_t* stat_vis;  // B (may be null)
-  uint32_t* stat_cmps; // B (may be null)
+  uint32_t* new_out;     // B x Rp
+  uint32_t* stat_vis;    // B (may be null)
+  uint32_t* stat_cmps;   // B (may be null)
+  uint32_t* vis_arena;   // per resident warp: vcap visited ids, then vcap distances
 };
 
+// The round's reverse edges grouped by target (see semisort.cuh): segment k
+// holds pairs [heads[k], heads[k+1]) of st (targets) / sv (keys b*Rp + j).
 struct ReverseScratch {
-  uint32_t* cnt;       // n, zero between rounds
-  uint32_t* cursor;    // n
-  uint32_t* touched;   // list of targets with incoming edges
-  uint32_t* seg_start; // per touched entry
-  uint32_t* keys;      // B*Rp segment keys (b*Rp + j)
-  uint32_t* counters;  // [0] touched, [1] big entries, [2] pruned groups, [3] prune cands
-  uint32_t* big;       // touched entries handled by the global-memory path
-  uint32_t* block_sums;// scan partials (kScanBlocks + 1)
-  uint32_t* gcand;     // global candidate workspace for the big path
-  float* gkey;
-  int* gleaf;          // 2x workspace for leaves + stack
-  uint64_t gcap;       // candidate capacity of the big path
+  const uint32_t* st;
+  const uint32_t* sv;
+  const uint32_t* heads;
+  uint32_t* counters;  // [0] pairs V [1] segments T [2] pruned groups [3] prune cands
+                       // [4] big segments [5] largest big candidate list
+  uint32_t* big;       // segments for the CTA path
+  // CTA path workspace, one slice per CTA (kBigSlots slices of gcap candidates):
+  uint32_t* gcand;     // gcap ids
+  float* gkey;         // gcap distances
+  int* gpos;           // 2*gcap rank scratch
+  uint32_t* gbits;     // gcap/32 + 2 leaf bitmap words
+  int* granges;        // 3*(gcap/8 + 64) short-range records
+  uint64_t gcap;
 };
 
 constexpr int kScanBlocks = 512;
 // stack room of the sort emulation for any list length below 2^32
 constexpr int kGlobalStackInts = 3 * (2 * 32 + 4);
-constexpr uint32_t kRevCandCap = 512;   // shared-memory candidate capacity per target
+constexpr uint32_t kRevCandCap = 512;   // per-warp shared-memory candidates (reverse)
 constexpr uint32_t kRevWarps = 4;       // warps per CTA of the reverse kernel
+constexpr uint32_t kBigThreads = 512;   // threads per CTA of the big-target path
+constexpr uint32_t kBigSlots = 148;     // CTAs (and workspace slices) of the big-target path
 
 void launch_search_prune(const IndexView& ix, const RoundArgs& ra, const WarpLayout& lay,
                          int warps_per_cta, int grid, cudaStream_t st);
 void launch_apply_rows(const IndexView& ix, const RoundArgs& ra, cudaStream_t st);
+// append-or-prune per target over the segments the semisort produced
 void launch_reverse(const IndexView& ix, const RoundArgs& ra, const ReverseScratch& rs,
                     cudaStream_t st, int sm_count);
-void launch_reverse_big(const IndexView& ix, const RoundArgs& ra, const ReverseScratch& rs,
-                        uint32_t slots, cudaStream_t st);
 
 struct QueryArgs {
   const uint8_t* queries;  // device rows, stride qstride (zero padded to 16 bytes)
@@ -108,7 +116,8 @@ struct BeamArgs {
   uint32_t* vis_ids; float* vis_d; uint32_t* vis_n;  // nq x vcap
   uint32_t* cmps;
 };
-void launch_beam(const IndexView& ix, const BeamArgs& ba, const WarpLayout& lay, cudaStream_t st);
+void launch_beam(const IndexView& ix, const BeamArgs& ba, const WarpLayout& lay, int grid,
+                 cudaStream_t st);
 
 // robustPrune on explicit candidate lists (kernel-level parity tests)
 struct PruneArgs {
@@ -119,9 +128,9 @@ struct PruneArgs {
   const float* cand_d;
   double alpha;
   uint32_t* out;              // ntasks x Rp
-  // workspace: gcand/gkey hold offsets[ntasks] + ntasks*Rp entries, gleaf twice
-  // that plus ntasks*kGlobalStackInts
-  uint32_t* gcand; float* gkey; int* gleaf;
+  // workspace: gcand/gkey hold W = offsets[ntasks] + ntasks*Rp entries, gws
+  // 3*W + ntasks*kGlobalStackInts ints
+  uint32_t* gcand; float* gkey; int* gws;
 };
 void launch_prune_tasks(const IndexView& ix, const PruneArgs& pa, cudaStream_t st);
 

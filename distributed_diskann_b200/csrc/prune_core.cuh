@@ -1,8 +1,9 @@
 // Warp-cooperative robustPrune (include/index.h:63-123; src/bsp_index.hpp:483-545).
 //
 //  1. the candidate list (ids + distances to p) is ordered exactly as the
-//     reference's std::sort orders it (sort_emul.cuh: lane 0 replays the
-//     partition phase, then every lane finishes whole leaves);
+//     reference's std::sort orders it (sort_emul.cuh): the introsort
+//     partition phase is replayed with each Hoare partition done in parallel
+//     by rank pairing, then every lane finishes whole leaves;
 //  2. greedy selection: walk the sorted list, skip p and removed entries,
 //     select p*, and remove every later p' with alpha * d(p*, p') <= d(p, p')
 //     (alpha is a double in the reference, so the test is done in double).
@@ -13,24 +14,193 @@
 
 namespace ddk {
 
+__device__ __forceinline__ uint32_t lanemask_lt_() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
 struct PruneSmem {
-  uint32_t* cid;   // candidate ids (DD_NONE = removed)
-  float* ckey;     // distance to p
-  int* leaf_lo;    // leaf ranges of the sort emulation (capacity = candidates)
-  int* leaf_hi;
-  int* stack;      // ddsort::stack_ints(capacity) ints
-  int* scalar;     // one shared int
+  uint32_t* cid;      // candidate ids (DD_NONE = removed)
+  float* ckey;        // distance to p
+  uint32_t* leafbits; // leaf starts of the sort emulation, (capacity + 31) / 32 words
+  int* stack;         // ddsort::stack_ints(capacity) ints
+  int* posL;          // rank-pairing scratch, capacity ints each
+  int* posR;
 };
 
-// Orders cid/ckey[0, m) exactly like std::sort with the distance-only comparator.
+// bytes of the leaf bitmap + stack + rank scratch for `cap` candidates (16-byte multiple)
+__host__ __device__ inline uint32_t prune_ws_bytes(uint32_t cap) {
+  uint32_t b = ((cap + 31) / 32) * 4 + 4u * (uint32_t)ddsort::stack_ints((int)cap) + 8u * cap;
+  return (b + 15) & ~15u;
+}
+
+__device__ __forceinline__ PruneSmem prune_ws(uint32_t* cid, float* ckey, uint8_t* ws, uint32_t cap) {
+  PruneSmem p;
+  p.cid = cid;
+  p.ckey = ckey;
+  p.leafbits = (uint32_t*)ws;
+  p.stack = (int*)(ws + ((cap + 31) / 32) * 4);
+  p.posL = p.stack + ddsort::stack_ints((int)cap);
+  p.posR = p.posL + cap;
+  return p;
+}
+
+// One Hoare partition of [first, last) around the pivot at `pivot` (= first-1),
+// done by the warp: the k-th "not less" position from the left is swapped
+// with the k-th "not greater" position from the right for every k where the
+// former is left of the latter (ddsort::partition_by_rank_pairing).
+__device__ __forceinline__ int warp_partition_rank(const ddsort::Arr<uint32_t>& A, int first,
+                                                   int last, int pivot, int* posL, int* posR) {
+  const uint32_t FULL = 0xffffffffu;
+  const int lane = (int)lane_id();
+  const float pk = A.key[pivot];
+  int nL = 0;
+  for (int base = first; base < last; base += 32) {
+    const int i = base + lane;
+    const bool f = i < last && !(A.key[i] < pk);
+    const uint32_t b = __ballot_sync(FULL, f);
+    if (f) posL[nL + __popc(b & lanemask_lt_())] = i;
+    nL += __popc(b);
+  }
+  int nR = 0;
+  for (int base = last - 1; base >= pivot; base -= 32) {
+    const int i = base - lane;
+    const bool f = i >= pivot && !(pk < A.key[i]);
+    const uint32_t b = __ballot_sync(FULL, f);
+    if (f) posR[nR + __popc(b & lanemask_lt_())] = i;
+    nR += __popc(b);
+  }
+  __syncwarp();
+  const int lim = nL < nR ? nL : nR;
+  int K = 0;
+  for (int kb = 0; kb < lim; kb += 32) {  // posL[k] < posR[k] holds for a prefix of k
+    const int k = kb + lane;
+    const uint32_t b = __ballot_sync(FULL, k < lim && posL[k] < posR[k]);
+    K += __popc(b);
+    if (b != FULL) break;
+  }
+  for (int k = lane; k < K; k += 32) A.swap(posL[k], posR[k]);
+  __syncwarp();
+  if (K == 0) return posL[0];
+  const int a = K < nL ? posL[K] : last;
+  const int r = posR[K - 1];
+  return a < r ? a : r;
+}
+
+// The introsort partition phase of one range [first0, last0) with the
+// remaining depth budget depth0, replayed by a warp: median-of-three and the
+// heap fallback on lane 0, each partition in parallel; leaf starts are marked
+// in `bits` (atomically when other warps mark neighbouring ranges).  posL /
+// posR need room for last0 - first0 entries; the stack for
+// 3 * (depth0 + 2) ints.
+__device__ __forceinline__ void warp_partition_loop(const ddsort::Arr<uint32_t>& A, int first0,
+                                                    int last0, int depth0, int* stack,
+                                                    uint32_t* bits, int* posL, int* posR,
+                                                    bool atomic_bits) {
+  const uint32_t lane = lane_id();
+  if (lane == 0) {
+    stack[0] = first0;
+    stack[1] = last0;
+    stack[2] = depth0;
+  }
+  int sp = 3;
+  __syncwarp();
+  while (sp > 0) {
+    int depth = stack[sp - 1], last = stack[sp - 2], first = stack[sp - 3];
+    sp -= 3;
+    __syncwarp();
+    while (last - first > ddsort::kThreshold) {
+      if (depth == 0) {
+        if (lane == 0) ddsort::heap_sort_range(A, first, last);
+        __syncwarp();
+        break;
+      }
+      --depth;
+      const int mid = first + (last - first) / 2;
+      if (lane == 0) ddsort::move_median_to_first(A, first, first + 1, mid, last - 1);
+      __syncwarp();
+      const int cut = warp_partition_rank(A, first + 1, last, first, posL, posR);
+      if (lane == 0) {
+        stack[sp] = cut;
+        stack[sp + 1] = last;
+        stack[sp + 2] = depth;
+      }
+      sp += 3;
+      last = cut;
+      __syncwarp();
+    }
+    if (lane == 0) {
+      if (atomic_bits) atomicOr(&bits[first >> 5], 1u << (first & 31));
+      else bits[first >> 5] |= 1u << (first & 31);
+    }
+    __syncwarp();
+  }
+}
+
+// Orders cid/ckey[0, m) exactly like std::sort with the distance-only
+// comparator: the warp replays the partition phase, marking leaf starts in a
+// bitmap; then the lanes finish the leaves in parallel.
 __device__ __forceinline__ void warp_std_sort(const PruneSmem& S, uint32_t m) {
   const uint32_t lane = lane_id();
   ddsort::Arr<uint32_t> A{S.cid, S.ckey};
-  if (lane == 0) S.scalar[0] = ddsort::partition_phase(A, (int)m, S.stack, S.leaf_lo, S.leaf_hi);
+  const uint32_t nw = (m + 31) / 32;
+  for (uint32_t w = lane; w < nw; w += 32) S.leafbits[w] = 0;
   __syncwarp();
-  const int nl = S.scalar[0];
-  for (int i = (int)lane; i < nl; i += 32) ddsort::insertion_sort_range(A, S.leaf_lo[i], S.leaf_hi[i]);
+  if (m > 0)
+    warp_partition_loop(A, 0, (int)m, 2 * ddsort::floor_log2((int)m), S.stack, S.leafbits, S.posL,
+                        S.posR, false);
+  for (uint32_t i = lane; i < m; i += 32)
+    if (S.leafbits[i >> 5] & (1u << (i & 31)))
+      ddsort::insertion_sort_range(A, (int)i, ddsort::leaf_end(S.leafbits, (int)i, (int)m));
   __syncwarp();
+}
+
+// CTA-wide sum (all threads call it; sh: 32 words)
+__device__ __forceinline__ uint32_t cta_reduce_add(uint32_t v, uint32_t* sh) {
+  uint32_t tot;
+  cta_scan_excl(v, &tot, sh);
+  return tot;
+}
+
+// One Hoare partition (rank pairing) done by the whole CTA; the pivot value
+// must be in place at `pivot` (= first - 1) before the call.
+__device__ __forceinline__ int cta_partition_rank(const ddsort::Arr<uint32_t>& A, int first,
+                                                  int last, int pivot, int* posL, int* posR,
+                                                  uint32_t* sh) {
+  const int NT = (int)blockDim.x, tid = (int)threadIdx.x;
+  const float pk = A.key[pivot];
+  // left stops, ascending: contiguous chunks per thread
+  const int n = last - first;
+  const int ch = (n + NT - 1) / NT;
+  const int lo = first + tid * ch, hi = min(last, lo + ch);
+  uint32_t c = 0;
+  for (int i = lo; i < hi; i++) c += !(A.key[i] < pk) ? 1u : 0u;
+  uint32_t nL;
+  uint32_t j = cta_scan_excl(c, &nL, sh);
+  for (int i = lo; i < hi; i++)
+    if (!(A.key[i] < pk)) posL[j++] = i;
+  // right stops, descending over [pivot, last)
+  const int nr = last - pivot;
+  const int ch2 = (nr + NT - 1) / NT;
+  const int q0 = tid * ch2, q1 = min(nr, q0 + ch2);
+  c = 0;
+  for (int q = q0; q < q1; q++) c += !(pk < A.key[last - 1 - q]) ? 1u : 0u;
+  uint32_t nR;
+  j = cta_scan_excl(c, &nR, sh);
+  for (int q = q0; q < q1; q++)
+    if (!(pk < A.key[last - 1 - q])) posR[j++] = last - 1 - q;
+  __syncthreads();
+  const int lim = (int)min(nL, nR);
+  c = 0;
+  for (int k = tid; k < lim; k += NT) c += posL[k] < posR[k] ? 1u : 0u;
+  const int K = (int)cta_reduce_add(c, sh);  // the pairs with posL < posR form a prefix
+  for (int k = tid; k < K; k += NT) A.swap(posL[k], posR[k]);
+  __syncthreads();
+  if (K == 0) return posL[0];
+  const int a = K < (int)nL ? posL[K] : last;
+  const int r = posR[K - 1];
+  return a < r ? a : r;
 }
 
 // Greedy selection over the sorted candidates; writes the selected ids to

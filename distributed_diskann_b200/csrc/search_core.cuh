@@ -14,26 +14,26 @@
 //    visited                                                         (:108, :175-178)
 //
 // Parallel forms of the sequential steps:
-//  * "visited" is a flag bit in the frontier id (ids are unique in the
-//    frontier, so set_difference(frontier, visited) is "flag clear").  A node
-//    dropped from the frontier after its visit is remembered in an "evicted"
-//    list; if it ever re-enters (possible only in query mode, after a k-cut)
-//    it re-enters flagged, as set_difference would treat it.
+//  * "visited" is a flag bit in the frontier id.  Within a run of identical
+//    frontier entries the flagged copies come first, so the first unflagged
+//    entry is the first element of set_difference(frontier, visited) even
+//    when the lists are multisets (rows holding an id twice, as two-pass
+//    builds produce).  Visited entries dropped from the frontier are kept in
+//    an "evicted" list so a re-entering copy is flagged as set_difference
+//    would (only possible in query mode, after a k-cut).
 //  * the hash filter is replayed exactly: lanes whose ids fall in the same
 //    slot are grouped with __match_any_sync; within a group the table value a
 //    lane sees is the id of the previous lane in neighbour order (or the table
-//    entry), and the last lane of the group writes the slot.
-//  * set_union + trim: candidates are ranked by (dist, id), duplicates of
-//    frontier entries dropped (set_union keeps the frontier's copy), and every
-//    element moves to its merged position; positions >= L are dropped.
+//    entry), and the last lane of the group writes the slot.  The table lives
+//    in a per-warp slice of global memory (L1/L2 resident).
+//  * set_union + trim: candidates are ranked by (dist, id), the copies
+//    set_union adds are kept, and every element moves to its merged position;
+//    positions >= L are dropped.
 #pragma once
 #include "dd_common.cuh"
 #include "kernels.cuh"
 
 namespace ddk {
-
-constexpr uint32_t kMaxFrPerLane = kMaxL / 32;
-constexpr uint32_t kMaxCandPerLane = kMaxRp / 32;
 
 struct SearchSmem {
   uint8_t* qv;        // query vector (16-byte aligned, zero padded)
@@ -46,7 +46,7 @@ struct SearchSmem {
   uint32_t* vis_id;   // visited list in visit order (keep_visited), capacity vcap
   float* vis_d;
   uint32_t* ev_id;    // visited ids pushed out of the frontier (query_mode), capacity vcap
-  uint32_t* hash;     // 2^bits slots
+  uint32_t* hash;     // 2^bits slots (global memory, this warp's slice)
 };
 
 struct SearchParams {
@@ -103,13 +103,18 @@ __device__ __forceinline__ float point_dist(const SearchParams& P, const uint8_t
 // Runs one beam search on the warp.  `qv` must already hold the query.
 // self_id: the id the reference skips as p.id() (the point itself in the
 // build, the query's index in searchAll).
-template <int DT, int MT>
+// FPL: frontier entries per lane (L <= 32*FPL); CPL: 32-lane chunks of a row (Rp <= 32*CPL).
+template <int DT, int MT, int FPL, int CPL>
 __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S, uint64_t self_id) {
   const uint32_t lane = lane_id();
   const uint32_t FULL = 0xffffffffu;
   const uint32_t nslots = 1u << P.hbits;
   const uint32_t hmask = nslots - 1;
-  for (uint32_t i = lane; i < nslots; i += 32) S.hash[i] = DD_NONE;
+  {
+    uint4* h4 = (uint4*)S.hash;
+    const uint4 none = make_uint4(DD_NONE, DD_NONE, DD_NONE, DD_NONE);
+    for (uint32_t i = lane; i < nslots / 4; i += 32) h4[i] = none;
+  }
   if (lane == 0) {
     S.fr_id[0] = P.start;
     S.fr_d[0] = point_dist<DT, MT>(P, S.qv, P.start);
@@ -121,7 +126,21 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
   uint32_t cmps = 1;       // dist to the start point
   uint64_t num_visited = 0;
   const float int_max_f = 2147483648.0f;  // (float)std::numeric_limits<int>::max()
-  const uint32_t dl = P.degree_limit;
+  const uint32_t dl = min(P.degree_limit, P.Rp);
+  // The row of the node expected to be visited next is loaded while the
+  // current step is still merging (a speculative load: it is used only if
+  // that node is indeed the one visited next).
+  uint32_t pred = DD_NONE;
+  uint32_t a_pre[CPL];
+  auto prefetch_row = [&](uint32_t node) {
+    pred = node;
+    const uint32_t* prow = P.graph + (uint64_t)node * P.Rp;
+#pragma unroll
+    for (int t = 0; t < CPL; t++) {
+      uint32_t j = 32 * t + lane;
+      a_pre[t] = (j < dl) ? __ldg(prow + j) : DD_NONE;
+    }
+  };
 
   while (num_visited < P.limit) {
     // ---- closest unvisited frontier entry
@@ -135,6 +154,20 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
     if (cur_pos < 0) break;
     const uint32_t cur = S.fr_id[cur_pos];
     const float cur_d = S.fr_d[cur_pos];
+    const float cutoff = (fr_n < P.L) ? int_max_f : S.fr_d[fr_n - 1];
+    // the row of the node being visited: all chunks loaded up front
+    uint32_t a[CPL];
+    if (cur == pred) {
+#pragma unroll
+      for (int t = 0; t < CPL; t++) a[t] = a_pre[t];
+    } else {
+      const uint32_t* row = P.graph + (uint64_t)cur * P.Rp;
+#pragma unroll
+      for (int t = 0; t < CPL; t++) {
+        uint32_t j = 32 * t + lane;
+        a[t] = (j < dl) ? __ldg(row + j) : DD_NONE;
+      }
+    }
     __syncwarp();
     if (lane == 0) {
       S.fr_id[cur_pos] = cur | DD_VBIT;
@@ -149,44 +182,64 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
     }
     if (P.keep_visited && vis_n < P.vcap) vis_n++;
     num_visited++;
-    const float cutoff = (fr_n < P.L) ? int_max_f : S.fr_d[fr_n - 1];
-    __syncwarp();
+    // the next unvisited entry after cur: visited next unless a new candidate beats it
+    int nxt_pos = -1;
+    for (uint32_t base = (uint32_t)(cur_pos + 1) & ~31u; base < fr_n; base += 32) {
+      uint32_t i = base + lane;
+      bool unv = (i > (uint32_t)cur_pos) && (i < fr_n) && !(S.fr_id[i] & DD_VBIT);
+      uint32_t b = __ballot_sync(FULL, unv);
+      if (b) { nxt_pos = (int)(base + __ffs(b) - 1); break; }
+    }
 
-    // ---- expand: hash filter (exact replay), distances, compaction
-    const uint32_t* row = P.graph + (uint64_t)cur * P.Rp;
-    uint32_t nc = 0;
-    for (uint32_t base = 0; base < P.Rp && base < dl; base += 32) {
-      uint32_t j = base + lane;
-      uint32_t a = (j < P.Rp && j < dl) ? __ldg(row + j) : DD_NONE;
-      if (a != DD_NONE && a >= P.n) {
+    // ---- hash filter, replayed chunk by chunk in neighbour order
+    bool keep[CPL];
+#pragma unroll
+    for (int t = 0; t < CPL; t++) {
+      uint32_t at = a[t];
+      if (at != DD_NONE && at >= P.n) {
         dd_set_error(P.err, DD_EBAD_ID);
-        a = DD_NONE;
+        at = DD_NONE;
+        a[t] = DD_NONE;
       }
-      bool part = (a != DD_NONE) && ((uint64_t)a != self_id);
-      uint32_t loc = part ? (uint32_t)(dd_hash64(a) & hmask) : (0x80000000u | lane);
+      bool part = (at != DD_NONE) && ((uint64_t)at != self_id);
+      uint32_t loc = part ? (uint32_t)(dd_hash64(at) & hmask) : (0x80000000u | lane);
       uint32_t grp = __match_any_sync(FULL, loc);
       uint32_t before = grp & lanemask_lt();
       uint32_t tval = part ? S.hash[loc] : DD_NONE;
-      uint32_t prev_a = __shfl_sync(FULL, a, before ? 31 - __clz(before) : lane);
+      uint32_t prev_a = __shfl_sync(FULL, at, before ? 31 - __clz(before) : lane);
       uint32_t seen_val = before ? prev_a : tval;
-      bool keep = part && (seen_val != a);
+      keep[t] = part && (seen_val != at);
       __syncwarp();
-      if (part && (grp & lanemask_gt()) == 0) S.hash[loc] = a;
+      if (part && (grp & lanemask_gt()) == 0) S.hash[loc] = at;
       __syncwarp();
-      float dist = 0.f;
-      if (keep) dist = point_dist<DT, MT>(P, S.qv, a);
-      cmps += __popc(__ballot_sync(FULL, keep));
-      bool pass = keep && (dist < cutoff);
+    }
+
+    // ---- distances of the kept neighbours (all chunks' loads interleaved)
+    float dist[CPL];
+    {
+      const uint8_t* rows[CPL];
+#pragma unroll
+      for (int t = 0; t < CPL; t++) rows[t] = P.points + (uint64_t)(keep[t] ? a[t] : 0) * P.stride;
+      DistRows<DT, MT, CPL>::eval(S.qv, rows, keep, P.d, dist);
+    }
+    uint32_t nc = 0;
+#pragma unroll
+    for (int t = 0; t < CPL; t++) {
+      cmps += __popc(__ballot_sync(FULL, keep[t]));
+      bool pass = keep[t] && (dist[t] < cutoff);
       uint32_t pb = __ballot_sync(FULL, pass);
       if (pass) {
         uint32_t pos = nc + __popc(pb & lanemask_lt());
-        S.c_id[pos] = a;
-        S.c_d[pos] = dist;
+        S.c_id[pos] = a[t];
+        S.c_d[pos] = dist[t];
       }
       nc += __popc(pb);
     }
     __syncwarp();
-    if (nc == 0) continue;
+    if (nc == 0) {
+      if (nxt_pos >= 0) prefetch_row(S.fr_id[nxt_pos]);
+      continue;
+    }
 
     // ---- rank candidates by (dist, id).  The same id can be kept twice in one
     // step (a row holding it twice, with a colliding id between the copies,
@@ -208,11 +261,11 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
     // copies, the candidate copies k >= m are added, after the frontier's copies.
     // A re-entering copy counts as visited while k < (visits of the value):
     // set_difference(frontier, visited) is a multiset difference too.
-    bool a_ok[kMaxCandPerLane];
-    uint32_t a_id[kMaxCandPerLane], a_ub[kMaxCandPerLane];
-    float a_d[kMaxCandPerLane];
+    bool a_ok[CPL];
+    uint32_t a_id[CPL], a_ub[CPL];
+    float a_d[CPL];
 #pragma unroll
-    for (uint32_t t = 0; t < kMaxCandPerLane; t++) {
+    for (int t = 0; t < CPL; t++) {
       uint32_t i = lane + 32 * t;
       a_ok[t] = false;
       a_id[t] = 0;
@@ -251,7 +304,7 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
     __syncwarp();
     uint32_t nkeep = 0;
 #pragma unroll
-    for (uint32_t t = 0; t < kMaxCandPerLane; t++) {
+    for (int t = 0; t < CPL; t++) {
       uint32_t ob = __ballot_sync(FULL, a_ok[t]);
       if (a_ok[t]) {
         uint32_t pos = nkeep + __popc(ob & lanemask_lt());
@@ -263,37 +316,44 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
       nkeep += __popc(ob);
     }
     __syncwarp();
+    {
+      // expected next node: the better of the best new candidate and nxt_pos
+      uint32_t nid = DD_NONE;
+      if (nkeep > 0 && !(S.c_id[0] & DD_VBIT)) nid = S.c_id[0];
+      if (nxt_pos >= 0 &&
+          (nid == DD_NONE || !pair_less(S.c_d[0], nid, S.fr_d[nxt_pos], S.fr_id[nxt_pos])))
+        nid = S.fr_id[nxt_pos];
+      if (nid != DD_NONE) prefetch_row(nid);
+    }
     if (nkeep == 0) continue;
 
-    // ---- merge: frontier entry i moves to i + #(candidates before it)
+    // ---- merge: frontier entry i moves to i + #(kept candidates placed before
+    // it) = i + #{j : ub_j <= i}; candidate j moves to j + ub_j
     const uint32_t new_n = min(P.L, fr_n + nkeep);
-    uint32_t my_id[kMaxFrPerLane];
-    float my_d[kMaxFrPerLane];
-    uint32_t my_pos[kMaxFrPerLane];
+    uint32_t my_id[FPL], my_pos[FPL];
+    float my_d[FPL];
 #pragma unroll
-    for (uint32_t t = 0; t < kMaxFrPerLane; t++) {
+    for (int t = 0; t < FPL; t++) {
       uint32_t i = lane + 32 * t;
       my_pos[t] = DD_NONE;
       my_id[t] = 0;
       my_d[t] = 0.f;
       if (i < fr_n) {
-        uint32_t fi = S.fr_id[i];
-        float fd = S.fr_d[i];
-        uint32_t lo = 0, hi = nkeep;  // candidates strictly before this entry
+        uint32_t lo = 0, hi = nkeep;
         while (lo < hi) {
           uint32_t mid = (lo + hi) >> 1;
-          if (pair_less(S.c_d[mid], S.c_id[mid] & ~DD_VBIT, fd, fi & ~DD_VBIT)) lo = mid + 1;
+          if (S.s_id[mid] <= i) lo = mid + 1;
           else hi = mid;
         }
-        my_id[t] = fi;
-        my_d[t] = fd;
+        my_id[t] = S.fr_id[i];
+        my_d[t] = S.fr_d[i];
         my_pos[t] = i + lo;
       }
     }
-    uint32_t c_ids[kMaxCandPerLane], c_pos[kMaxCandPerLane];
-    float c_ds[kMaxCandPerLane];
+    uint32_t c_ids[CPL], c_pos[CPL];
+    float c_ds[CPL];
 #pragma unroll
-    for (uint32_t t = 0; t < kMaxCandPerLane; t++) {
+    for (int t = 0; t < CPL; t++) {
       uint32_t j = lane + 32 * t;
       c_pos[t] = DD_NONE;
       c_ids[t] = 0;
@@ -306,14 +366,14 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
     }
     __syncwarp();
 #pragma unroll
-    for (uint32_t t = 0; t < kMaxFrPerLane; t++) {
+    for (int t = 0; t < FPL; t++) {
       if (my_pos[t] < new_n) {
         S.fr_id[my_pos[t]] = my_id[t];
         S.fr_d[my_pos[t]] = my_d[t];
       }
     }
 #pragma unroll
-    for (uint32_t t = 0; t < kMaxCandPerLane; t++) {
+    for (int t = 0; t < CPL; t++) {
       if (c_pos[t] < new_n) {
         S.fr_id[c_pos[t]] = c_ids[t];
         S.fr_d[c_pos[t]] = c_ds[t];
@@ -322,7 +382,7 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
     if (P.query_mode) {
       // visited entries pushed off the end are remembered (in frontier order)
 #pragma unroll
-      for (uint32_t t = 0; t < kMaxFrPerLane; t++) {
+      for (int t = 0; t < FPL; t++) {
         bool ev = (my_pos[t] != DD_NONE) && (my_pos[t] >= new_n) && (my_id[t] & DD_VBIT);
         uint32_t eb = __ballot_sync(FULL, ev);
         if (ev) {

@@ -33,6 +33,15 @@ namespace ddsort {
 
 constexpr int kThreshold = 16;
 
+// count of trailing zero bits of a non-zero word
+DD_HD int ctz32(uint32_t w) {
+#ifdef __CUDA_ARCH__
+  return __ffs(w) - 1;
+#else
+  return __builtin_ctz(w);
+#endif
+}
+
 template <typename IdT>
 struct Arr {
   IdT* id;
@@ -78,6 +87,31 @@ DD_HD int unguarded_partition(const Arr<IdT>& A, int first, int last, int pivot)
     A.swap(first, last);
     ++first;
   }
+}
+
+// The same partition written as rank pairing, the form the parallel device
+// code uses.  With the pivot value pk at `pivot` == first - 1:
+//   left stops  l_1 < l_2 < ...  : positions in [first, last) with !(key < pk)
+//   right stops r_1 > r_2 > ...  : positions in [pivot, last) with !(pk < key)
+// the library swaps (l_k, r_k) for every k with l_k < r_k (K such pairs; the
+// positions it visits in between are never ones a swap already touched) and
+// returns min(l_{K+1}, r_K) (l_1 when K = 0; r_K when l_{K+1} does not exist).
+// posL / posR need room for last - pivot entries.
+template <typename IdT>
+DD_HD int partition_by_rank_pairing(const Arr<IdT>& A, int first, int last, int pivot, int* posL,
+                                    int* posR) {
+  const float pk = A.key[pivot];
+  int nL = 0, nR = 0;
+  for (int i = first; i < last; i++)
+    if (!(A.key[i] < pk)) posL[nL++] = i;
+  for (int i = last - 1; i >= pivot; i--)
+    if (!(pk < A.key[i])) posR[nR++] = i;
+  int K = 0;
+  while (K < nL && K < nR && posL[K] < posR[K]) K++;
+  for (int k = 0; k < K; k++) A.swap(posL[k], posR[k]);
+  if (K == 0) return posL[0];
+  int a = K < nL ? posL[K] : last;
+  return a < posR[K - 1] ? a : posR[K - 1];
 }
 
 // ---- heap fallback (make_heap + sort_heap over a whole range)
@@ -151,11 +185,70 @@ DD_HD void insertion_sort_range(const Arr<IdT>& A, int first, int last) {
   }
 }
 
-// Partition phase.  `stack` needs room for 2*(floor_log2(n)+2) ints; leaves
-// are appended to leaf_lo/leaf_hi (room for n entries) and their count returned.
-template <typename IdT>
-DD_HD int partition_phase(const Arr<IdT>& A, int n, int* stack, int* leaf_lo, int* leaf_hi) {
-  int nleaf = 0;
+// Leaf sinks of the partition phase.
+struct LeafList {  // explicit (lo, hi) pairs, room for n entries each
+  int* lo;
+  int* hi;
+  int n = 0;
+  DD_HD void add(int a, int b) { lo[n] = a; hi[n] = b; n++; }
+};
+struct LeafBits {  // one bit per position, set where a leaf starts ((n + 31) / 32 words)
+  uint32_t* bits;
+  int n = 0;
+  DD_HD void add(int a, int) { bits[a >> 5] |= 1u << (a & 31); n++; }
+};
+
+// end of the leaf starting at `lo` in a LeafBits bitmap of n positions
+DD_HD int leaf_end(const uint32_t* bits, int lo, int n) {
+  int p = lo + 1;
+  while (p < n) {
+    uint32_t w = bits[p >> 5] & (0xffffffffu << (p & 31));
+    if (w) {
+      int q = (p & ~31) + (int)ctz32(w);
+      return q < n ? q : n;
+    }
+    p = (p & ~31) + 32;
+  }
+  return n;
+}
+
+// Partition phase with the partition done by rank pairing (posL / posR need
+// room for n entries); must give exactly what partition_phase gives.
+template <typename IdT, typename Sink>
+DD_HD int partition_phase_rank(const Arr<IdT>& A, int n, int* stack, Sink& sink, int* posL,
+                               int* posR) {
+  if (n <= 0) return 0;
+  int sp = 0;
+  stack[sp++] = 0;
+  stack[sp++] = n;
+  stack[sp++] = 2 * floor_log2(n);
+  while (sp > 0) {
+    int depth = stack[--sp];
+    int last = stack[--sp];
+    int first = stack[--sp];
+    while (last - first > kThreshold) {
+      if (depth == 0) {
+        heap_sort_range(A, first, last);
+        break;
+      }
+      --depth;
+      int mid = first + (last - first) / 2;
+      move_median_to_first(A, first, first + 1, mid, last - 1);
+      int cut = partition_by_rank_pairing(A, first + 1, last, first, posL, posR);
+      stack[sp++] = cut;
+      stack[sp++] = last;
+      stack[sp++] = depth;
+      last = cut;
+    }
+    sink.add(first, last);
+  }
+  return sink.n;
+}
+
+// Partition phase.  `stack` needs stack_ints(n) ints; every leaf range is
+// passed to sink.add(lo, hi); returns the number of leaves.
+template <typename IdT, typename Sink>
+DD_HD int partition_phase(const Arr<IdT>& A, int n, int* stack, Sink& sink) {
   if (n <= 0) return 0;
   // each stack entry: (first, last, depth) packed as three ints
   int sp = 0;
@@ -181,11 +274,15 @@ DD_HD int partition_phase(const Arr<IdT>& A, int n, int* stack, int* leaf_lo, in
       stack[sp++] = depth;
       last = cut;
     }
-    leaf_lo[nleaf] = first;
-    leaf_hi[nleaf] = last;
-    nleaf++;
+    sink.add(first, last);
   }
-  return nleaf;
+  return sink.n;
+}
+
+template <typename IdT>
+DD_HD int partition_phase(const Arr<IdT>& A, int n, int* stack, int* leaf_lo, int* leaf_hi) {
+  LeafList s{leaf_lo, leaf_hi};
+  return partition_phase(A, n, stack, s);
 }
 
 // Whole std::sort on one thread: the CPU tests check this against std::sort.
@@ -193,6 +290,16 @@ template <typename IdT>
 DD_HD void introsort_emulated(const Arr<IdT>& A, int n, int* stack, int* leaf_lo, int* leaf_hi) {
   int nl = partition_phase(A, n, stack, leaf_lo, leaf_hi);
   for (int i = 0; i < nl; i++) insertion_sort_range(A, leaf_lo[i], leaf_hi[i]);
+}
+
+// Same with the leaves recorded in a bitmap and finished leaf by leaf.
+template <typename IdT>
+DD_HD void introsort_emulated_bits(const Arr<IdT>& A, int n, int* stack, uint32_t* bits) {
+  for (int w = 0; w < (n + 31) / 32; w++) bits[w] = 0;
+  LeafBits s{bits};
+  partition_phase(A, n, stack, s);
+  for (int i = 0; i < n; i++)
+    if (bits[i >> 5] & (1u << (i & 31))) insertion_sort_range(A, i, leaf_end(bits, i, n));
 }
 
 // stack ints needed by partition_phase for n elements

@@ -27,6 +27,26 @@ static int check(const std::vector<std::pair<unsigned, float>>& in, bool* heap_u
   }
   for (int i = 0; i < n; i++)
     if (id[i] != ref[i].first || key[i] != ref[i].second) return 1;
+  // the bitmap-leaf form used by the device prune must agree too
+  std::vector<unsigned> id2(n);
+  std::vector<float> key2(n);
+  for (int i = 0; i < n; i++) id2[i] = in[i].first, key2[i] = in[i].second;
+  std::vector<uint32_t> bits((n + 31) / 32 + 1);
+  ddsort::Arr<unsigned> B{id2.data(), key2.data()};
+  ddsort::introsort_emulated_bits(B, n, stack.data(), bits.data());
+  for (int i = 0; i < n; i++)
+    if (id2[i] != ref[i].first || key2[i] != ref[i].second) return 2;
+  // and the rank-pairing partition (the form the parallel device code uses)
+  std::vector<unsigned> id3(n);
+  std::vector<float> key3(n);
+  for (int i = 0; i < n; i++) id3[i] = in[i].first, key3[i] = in[i].second;
+  std::vector<int> posL(n + 1), posR(n + 1), lo3(n + 1), hi3(n + 1);
+  ddsort::Arr<unsigned> C{id3.data(), key3.data()};
+  ddsort::LeafList sink{lo3.data(), hi3.data()};
+  int nl3 = ddsort::partition_phase_rank(C, n, stack.data(), sink, posL.data(), posR.data());
+  for (int i = 0; i < nl3; i++) ddsort::insertion_sort_range(C, lo3[i], hi3[i]);
+  for (int i = 0; i < n; i++)
+    if (id3[i] != ref[i].first || key3[i] != ref[i].second) return 3;
   return 0;
 }
 
