@@ -62,6 +62,7 @@ SIGNATURES = {
     "dd_beam_search": (i32, [vp, vp, u64, u64, vp, u32, u32, dbl, u64, u32, u32, u32, vp, vp, vp,
                              vp, vp, vp, vp]),
     "dd_robust_prune": (i32, [vp, u32, vp, vp, vp, vp, dbl, vp, vp]),
+    "dd_robust_prune_noalloc": (i32, [vp, u32, vp, vp, u64, vp, vp, dbl, vp, i32]),
     "dd_groundtruth": (i32, [vp, vp, u64, u64, u32, vp, vp]),
     "dd_device_points": (vp, [vp]),
     "dd_device_row_stride": (u64, [vp]),

@@ -804,3 +804,12 @@ uint32_t dd_device_row_len(dd_index* h) { return h ? h->Rp : 0; }
 uint64_t dd_last_launch_count(dd_index* h) { return h ? h->launches : 0; }
 
 }  // extern "C"
+
+// ---- accessors for the other translation units of the library (internal.h)
+namespace ddk {
+IndexView internal_view(dd_index* h) { return view(h); }
+cudaStream_t internal_stream(dd_index* h) { return h->stream; }
+int internal_device(dd_index* h) { return h->device; }
+int internal_fail(dd_index* h, int code, const char* msg) { return fail(h, code, "%s", msg); }
+int internal_check_error_word(dd_index* h) { return check_error_word(h); }
+}  // namespace ddk

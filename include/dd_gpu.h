@@ -141,6 +141,28 @@ int dd_robust_prune(dd_index* h, uint32_t ntasks, const uint32_t* p, const uint6
                     const uint32_t* cand_ids, const float* cand_dists, double alpha,
                     uint32_t* out, uint32_t* out_len);
 
+/* dd_robust_prune without any device allocation (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc at this point: a
+ * process that reserved its device memory up front and forbids later
+ * allocation, or work issued on a stream under CUDA-graph capture.  All
+ * arguments are DEVICE pointers: p (ntasks), offsets (ntasks + 1, with
+ * offsets[ntasks] == total_cands), cand_ids / cand_dists (total_cands), and out
+ * (ntasks x dd_device_row_len(h) ids, each row padded with 0xFFFFFFFF).  The
+ * candidate workspace is a fixed device array inside the library, held by every
+ * GPU that loads it until the process exits: at most 2048 tasks and
+ * total_cands + ntasks * dd_device_row_len(h) <= 65536 slots, larger calls
+ * return DD_ERR_UNSUPPORTED.  The first call on a device looks up that array's
+ * device address; make it before any stream capture.  All calls on a device
+ * share the array: calls whose kernels overlap on the GPU race and must be
+ * serialized.  The kernel runs on the handle's stream; with synchronize != 0
+ * the call waits for it and reports invalid device inputs (ids >= n, bad
+ * offsets), otherwise those rows are left as padding and the handle's error
+ * word reports them at its next synchronizing call. */
+int dd_robust_prune_noalloc(dd_index* h, uint32_t ntasks, const uint32_t* p,
+                            const uint64_t* offsets, uint64_t total_cands,
+                            const uint32_t* cand_ids, const float* cand_dists, double alpha,
+                            uint32_t* out, int synchronize);
+
 /* brute-force k nearest neighbours (k <= 32): FP64 distances for float data,
  * exact integers for integer data; ties ordered by id */
 int dd_groundtruth(dd_index* h, const void* queries, uint64_t nq, uint64_t qstride, uint32_t k,
