@@ -3,12 +3,11 @@
 //
 // Some callers cannot call cudaMalloc while they run this step: a host that
 // has reserved all device memory up front and forbids allocation afterwards
-// (a serving process with a fixed budget), a caller working on a stream that
-// is being captured into a CUDA graph (cudaMalloc is not permitted during
-// capture), or a caller whose memory belongs to another allocator that must not
-// be bypassed.  For them this entry point takes device pointers for every
-// input and output and keeps its candidate workspace in the fixed-size
-// device array below, which every GPU that loads the library holds until the
+// (a serving process with a fixed budget: cudaMalloc may also synchronize the
+// device and stall its other streams), or a caller whose memory belongs to
+// another allocator that must not be bypassed.  For them this entry point
+// takes device pointers for every input and output and keeps its candidate
+// workspace in the fixed-size device array below, which every GPU that loads the library holds until the
 // process exits.
 //
 // The workspace is shared by all calls on a device and keeps the last call's

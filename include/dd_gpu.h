@@ -143,8 +143,10 @@ int dd_robust_prune(dd_index* h, uint32_t ntasks, const uint32_t* p, const uint6
 
 /* dd_robust_prune without any device allocation (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc at this point: a
- * process that reserved its device memory up front and forbids later
- * allocation, or work issued on a stream under CUDA-graph capture.  All
+ * serving process that reserved its whole device-memory budget at start-up
+ * and forbids later allocation (cudaMalloc may also synchronize the device),
+ * or a host whose device memory belongs to another allocator that must not be
+ * bypassed.  All
  * arguments are DEVICE pointers: p (ntasks), offsets (ntasks + 1, with
  * offsets[ntasks] == total_cands), cand_ids / cand_dists (total_cands), and out
  * (ntasks x dd_device_row_len(h) ids, each row padded with 0xFFFFFFFF).  The

@@ -1,9 +1,10 @@
 """dd_robust_prune_noalloc: the allocation-free variant of dd_robust_prune.
 
 It is meant for callers that cannot call cudaMalloc while the prune runs (a
-process with a fixed, pre-reserved device-memory budget, or work issued on a
-stream under CUDA-graph capture): every argument is a device pointer and the
-candidate workspace is a fixed device array inside the library.  This test
+process with a fixed, pre-reserved device-memory budget, or a host whose
+device memory belongs to another allocator): every argument is a device
+pointer and the candidate workspace is a fixed device array inside the
+library.  This test
 calls it through the C ABI twice in a row (the shared workspace keeps the
 previous call's contents) and checks both results against dd_robust_prune,
 which allocates its own workspace.  Ids must match exactly.  The file is
