@@ -53,7 +53,10 @@ WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, ui
   if (with_prune) {
     w.vis_id = w.vis_d = 0;  // global
     w.ws = off;
-    uint32_t pws = r16(4ull * w.ccap) * 2 + prune_ws_bytes(w.ccap);
+    // the selected rows of the register-row greedy share the prune workspace
+    const uint32_t nv = row_words16(d, dtype);
+    const uint32_t sel_bytes = nv <= reg_row_max_words(dtype) ? Rp * nv * 16u : 0u;
+    uint32_t pws = r16(4ull * w.ccap) * 2 + prune_ws_bytes_sel(w.ccap, sel_bytes);
     off += hash_bytes > pws ? hash_bytes : pws;
   } else {
     w.vis_id = off; off += r16(4ull * vcap);
@@ -88,6 +91,7 @@ __device__ __forceinline__ WarpPtrs carve_build(uint8_t* base, const WarpLayout&
   uint8_t* ws = base + w.ws;
   const uint32_t cb = r16(4ull * w.ccap);
   r.Pm = prune_ws((uint32_t*)ws, (float*)(ws + cb), ws + 2 * cb, w.ccap);
+  r.Pm.sel = (uint4*)(ws + 2 * cb + prune_sel_offset(w.ccap));
   return r;
 }
 
@@ -173,8 +177,12 @@ __global__ void __launch_bounds__(64, 6) k_search_prune(IndexView ix, RoundArgs 
     }
     __syncwarp();
     warp_std_sort(W.Pm, m);
-    warp_greedy_select<DT, MT>(ix.points, ix.stride, ix.d, p, W.Pm, m, ra.alpha, ix.R,
-                               ra.new_out + b * ix.Rp, ix.Rp);
+    if (row_words16(ix.d, DT) <= (uint32_t)RegRow<DT>::NVM)
+      warp_greedy_select_reg<DT, MT>(ix.points, ix.stride, ix.d, p, W.Pm, m, ra.alpha, ix.R,
+                                     ra.new_out + b * ix.Rp, ix.Rp, W.Pm.sel);
+    else
+      warp_greedy_select<DT, MT>(ix.points, ix.stride, ix.d, p, W.Pm, m, ra.alpha, ix.R,
+                                 ra.new_out + b * ix.Rp, ix.Rp);
     if (lane == 0) {
       if (ra.stat_vis) ra.stat_vis[b] = o.vis_n;
       if (ra.stat_cmps) ra.stat_cmps[b] = o.cmps;
@@ -197,14 +205,16 @@ __global__ void k_apply_rows(uint32_t* graph, const uint32_t* new_out, uint64_t 
 struct RevLayout {
   uint32_t tv, cid, ckey, ws, total;
 };
-__host__ __device__ inline RevLayout rev_layout(uint32_t d, int dtype) {
+__host__ __device__ inline RevLayout rev_layout(uint32_t d, int dtype, uint32_t Rp) {
   RevLayout r;
   uint32_t off = 0;
   uint32_t esz = dtype == DD_F32 ? 4 : 1;
+  const uint32_t nv = row_words16(d, dtype);
+  const uint32_t sel_bytes = nv <= reg_row_max_words(dtype) ? Rp * nv * 16u : 0u;
   r.tv = off; off += r16((uint64_t)d * esz);
   r.cid = off; off += r16(4ull * kRevCandCap);
   r.ckey = off; off += r16(4ull * kRevCandCap);
-  r.ws = off; off += prune_ws_bytes(kRevCandCap);
+  r.ws = off; off += prune_ws_bytes_sel(kRevCandCap, sel_bytes);
   r.total = off;
   return r;
 }
@@ -246,7 +256,11 @@ __device__ void reverse_one(const IndexView& ix, const RoundArgs& ra, const Reve
   __syncwarp();
   const uint32_t m = s + deg;
   warp_std_sort(Pm, m);
-  warp_greedy_select<DT, MT>(ix.points, ix.stride, ix.d, t, Pm, m, ra.alpha, ix.R, row, ix.Rp);
+  if (row_words16(ix.d, DT) <= (uint32_t)RegRow<DT>::NVM)
+    warp_greedy_select_reg<DT, MT>(ix.points, ix.stride, ix.d, t, Pm, m, ra.alpha, ix.R, row,
+                                   ix.Rp, Pm.sel);
+  else
+    warp_greedy_select<DT, MT>(ix.points, ix.stride, ix.d, t, Pm, m, ra.alpha, ix.R, row, ix.Rp);
   if (lane == 0) {
     atomicAdd(&rs.counters[2], 1u);
     atomicAdd(&rs.counters[3], m);
@@ -254,13 +268,14 @@ __device__ void reverse_one(const IndexView& ix, const RoundArgs& ra, const Reve
 }
 
 template <int DT, int MT>
-__global__ void __launch_bounds__(kRevWarps * 32) k_reverse(IndexView ix, RoundArgs ra, ReverseScratch rs) {
+__global__ void __launch_bounds__(kRevWarps * 32, 4) k_reverse(IndexView ix, RoundArgs ra, ReverseScratch rs) {
   extern __shared__ uint4 smem_raw[];
-  const RevLayout L = rev_layout(ix.d, DT);
+  const RevLayout L = rev_layout(ix.d, DT, ix.Rp);
   const uint32_t wic = threadIdx.x >> 5, lane = lane_id();
   uint8_t* base = (uint8_t*)smem_raw + (size_t)wic * L.total;
   PruneSmem Pm = prune_ws((uint32_t*)(base + L.cid), (float*)(base + L.ckey), base + L.ws,
                           kRevCandCap);
+  Pm.sel = (uint4*)(base + L.ws + prune_sel_offset(kRevCandCap));
   const uint32_t T = rs.counters[1];
   for (uint32_t k = blockIdx.x * kRevWarps + wic; k < T; k += gridDim.x * kRevWarps) {
     uint32_t start, end;
@@ -783,7 +798,7 @@ void launch_apply_rows(const IndexView& ix, const RoundArgs& ra, cudaStream_t st
 void launch_reverse(const IndexView& ix, const RoundArgs& ra, const ReverseScratch& rs,
                     cudaStream_t st, int sm_count) {
   if (!ra.B) return;
-  RevLayout L = rev_layout(ix.d, ix.dtype);
+  RevLayout L = rev_layout(ix.d, ix.dtype, ix.Rp);
   size_t sm = (size_t)L.total * kRevWarps;
   int rg = sm_count * 8;
 #define CALL(DT, MT)                                                                  \

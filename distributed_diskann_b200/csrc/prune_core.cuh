@@ -27,6 +27,7 @@ struct PruneSmem {
   int* stack;         // ddsort::stack_ints(capacity) ints
   int* posL;          // rank-pairing scratch, capacity ints each
   int* posR;
+  uint4* sel;         // selected rows of warp_greedy_select_reg (overlays posL/posR), or null
 };
 
 // bytes of the leaf bitmap + stack + rank scratch for `cap` candidates (16-byte multiple)
@@ -43,6 +44,7 @@ __device__ __forceinline__ PruneSmem prune_ws(uint32_t* cid, float* ckey, uint8_
   p.stack = (int*)(ws + ((cap + 31) / 32) * 4);
   p.posL = p.stack + ddsort::stack_ints((int)cap);
   p.posR = p.posL + cap;
+  p.sel = nullptr;
   return p;
 }
 
@@ -230,6 +232,170 @@ __device__ uint32_t warp_greedy_select(const uint8_t* points, uint64_t stride, u
   for (uint32_t j = nsel + lane; j < Rp; j += 32) out_row[j] = DD_NONE;
   __syncwarp();
   return nsel;
+}
+
+// ---------------------------------------------------------------------------
+// Greedy selection with register-resident candidate rows.
+//
+// warp_greedy_select reads a whole candidate row from global memory (L1/L2)
+// per lane for every selected p*, so each selection waits on a round of
+// scattered loads.  This form walks the sorted list in chunks of 32: lane j
+// loads candidate c0+j's row into registers once (NVM 16-byte words), tests it
+// against the rows selected in earlier chunks, then the chunk is selected in
+// order.  Selected rows are kept in shared memory (`sel`, Rp rows of nv
+// 16-byte words) and read by broadcast, so the inner loops make no global
+// loads.  A candidate is removed iff some selected p* before it has
+// alpha * d(p*, p') <= d(p, p'), which is exactly the reference's rule
+// (include/index.h:100-118): removal is monotone and selection of an entry
+// depends only on the earlier selections, so testing against all earlier
+// selected rows in any grouping gives the same result.  Distances are the
+// reference's arithmetic with p* as the first operand, like Dist::eval.
+// ---------------------------------------------------------------------------
+template <int DT, int MT, int NVM>
+__device__ __forceinline__ float dist_reg(const uint4* a, const uint4 (&b)[NVM], uint32_t d,
+                                          uint32_t nv) {
+  if (DT == DD_F32) {
+    float r = 0.f;
+#pragma unroll
+    for (int k = 0; k < NVM; k++) {
+      if ((uint32_t)k >= nv) break;
+      const uint4 xa = a[k];
+      const float x[4] = {__uint_as_float(xa.x), __uint_as_float(xa.y), __uint_as_float(xa.z),
+                          __uint_as_float(xa.w)};
+      const float y[4] = {__uint_as_float(b[k].x), __uint_as_float(b[k].y),
+                          __uint_as_float(b[k].z), __uint_as_float(b[k].w)};
+      const uint32_t i = 4u * (uint32_t)k;
+      if (MT == DD_L2) {
+        if (i + 3 < d) {  // NSGDist: groups of 4 summed left to right, then added
+          float d0 = __fsub_rn(x[0], y[0]), d1 = __fsub_rn(x[1], y[1]);
+          float d2 = __fsub_rn(x[2], y[2]), d3 = __fsub_rn(x[3], y[3]);
+          float s = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)),
+                                        __fmul_rn(d2, d2)),
+                              __fmul_rn(d3, d3));
+          r = __fadd_rn(r, s);
+        } else {  // the 0-3 element tail, one at a time
+#pragma unroll
+          for (int t = 0; t < 4; t++)
+            if (i + t < d) {
+              float d0 = __fsub_rn(x[t], y[t]);
+              r = __fadd_rn(r, __fmul_rn(d0, d0));
+            }
+        }
+      } else {
+#pragma unroll
+        for (int t = 0; t < 4; t++)
+          if (i + t < d) r = __fadd_rn(r, __fmul_rn(x[t], y[t]));
+      }
+    }
+    return MT == DD_L2 ? r : -r;
+  } else {
+    uint32_t u = 0;
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < NVM; k++) {
+      if ((uint32_t)k >= nv) break;
+      const uint4 x = a[k];
+      const uint4 y = b[k];
+      if (MT == DD_L2) {
+        uint32_t s;
+        s = absdiff4<DT>(x.x, y.x); u = __dp4a(s, s, u);
+        s = absdiff4<DT>(x.y, y.y); u = __dp4a(s, s, u);
+        s = absdiff4<DT>(x.z, y.z); u = __dp4a(s, s, u);
+        s = absdiff4<DT>(x.w, y.w); u = __dp4a(s, s, u);
+      } else if (DT == DD_U8) {
+        u = __dp4a(x.x, y.x, u); u = __dp4a(x.y, y.y, u);
+        u = __dp4a(x.z, y.z, u); u = __dp4a(x.w, y.w, u);
+      } else {
+        v = __dp4a((int)x.x, (int)y.x, v); v = __dp4a((int)x.y, (int)y.y, v);
+        v = __dp4a((int)x.z, (int)y.z, v); v = __dp4a((int)x.w, (int)y.w, v);
+      }
+    }
+    if (MT == DD_L2) return __int2float_rn((int)u);
+    return DT == DD_U8 ? -__int2float_rn((int)u) : -__int2float_rn(v);
+  }
+}
+
+// 16-byte words of a padded point row, and the largest row the register form
+// takes (128 bytes for integer data, 256 bytes for float data)
+__host__ __device__ inline uint32_t row_words16(uint32_t d, int dtype) {
+  return (d * (dtype == DD_F32 ? 4u : 1u) + 15u) / 16u;
+}
+template <int DT>
+struct RegRow { static constexpr int NVM = (DT == DD_F32) ? 16 : 8; };
+__host__ __device__ inline uint32_t reg_row_max_words(int dtype) {
+  return dtype == DD_F32 ? 16u : 8u;
+}
+
+template <int DT, int MT>
+__device__ uint32_t warp_greedy_select_reg(const uint8_t* points, uint64_t stride, uint32_t d,
+                                           uint32_t p, const PruneSmem& S, uint32_t m,
+                                           double alpha, uint32_t R, uint32_t* out_row,
+                                           uint32_t Rp, uint4* sel) {
+  constexpr int NVM = RegRow<DT>::NVM;
+  const uint32_t FULL = 0xffffffffu;
+  const uint32_t lane = lane_id();
+  const uint32_t nv = row_words16(d, DT);
+  uint32_t nsel = 0;
+  for (uint32_t c0 = 0; c0 < m && nsel < R; c0 += 32) {
+    const uint32_t j = c0 + lane;
+    const uint32_t cj = j < m ? S.cid[j] : DD_NONE;
+    bool alive = cj != DD_NONE && cj != p;
+    const double kj = alive ? (double)S.ckey[j] : 0.0;
+    uint4 row[NVM];
+#pragma unroll
+    for (int k = 0; k < NVM; k++) row[k] = make_uint4(0, 0, 0, 0);
+    if (alive) {
+      const uint4* src = (const uint4*)(points + (uint64_t)cj * stride);
+#pragma unroll
+      for (int k = 0; k < NVM; k++)
+        if ((uint32_t)k < nv) row[k] = __ldg(src + k);
+    }
+    // occlusion by the rows selected in earlier chunks
+    for (uint32_t s = 0; s < nsel; s++) {
+      if (!__any_sync(FULL, alive)) break;
+      const float dsp = dist_reg<DT, MT, NVM>(sel + (uint64_t)s * nv, row, d, nv);
+      if (alive && __dmul_rn(alpha, (double)dsp) <= kj) alive = false;
+    }
+    // this chunk, in order
+    uint32_t rem = __ballot_sync(FULL, alive);
+    while (rem && nsel < R) {
+      const uint32_t i = (uint32_t)__ffs(rem) - 1;
+      uint4* dst = sel + (uint64_t)nsel * nv;
+      if (lane == i) {
+        out_row[nsel] = cj;
+#pragma unroll
+        for (int k = 0; k < NVM; k++)
+          if ((uint32_t)k < nv) dst[k] = row[k];
+      }
+      __syncwarp();
+      nsel++;
+      const bool later = alive && lane > i;
+      if (__any_sync(FULL, later)) {
+        const float dsp = dist_reg<DT, MT, NVM>(dst, row, d, nv);
+        if (later && __dmul_rn(alpha, (double)dsp) <= kj) alive = false;
+      }
+      rem = __ballot_sync(FULL, alive) & ~((2u << i) - 1u);
+    }
+    __syncwarp();
+  }
+  for (uint32_t j = nsel + lane; j < Rp; j += 32) out_row[j] = DD_NONE;
+  __syncwarp();
+  return nsel;
+}
+
+// byte offset of the (16-byte aligned) selected-row area inside a prune
+// workspace of `cap` candidates: it overlays the rank-pairing scratch, which
+// is dead once the sort is done
+__host__ __device__ inline uint32_t prune_sel_offset(uint32_t cap) {
+  uint32_t b = ((cap + 31) / 32) * 4 + 4u * (uint32_t)ddsort::stack_ints((int)cap);
+  return (b + 15) & ~15u;
+}
+// workspace bytes when the selected rows (sel_bytes) share it
+__host__ __device__ inline uint32_t prune_ws_bytes_sel(uint32_t cap, uint32_t sel_bytes) {
+  uint32_t a = prune_ws_bytes(cap);
+  uint32_t b = prune_sel_offset(cap) + sel_bytes;
+  b = (b + 15) & ~15u;
+  return a > b ? a : b;
 }
 
 // In-place ascending sort of (key, id) pairs by (key, id) on one warp:
