@@ -190,99 +190,55 @@ template <> struct Dist<DD_U8, DD_MIPS> : DistIntIP<DD_U8> {};
 template <int DT>
 struct ElemSize { static constexpr int v = (DT == DD_F32) ? 4 : 1; };
 
-// Distances from `a` to up to C rows at once (row t used when act[t]); the
-// loads of the C rows are interleaved so their latencies overlap.  Each row's
-// arithmetic is exactly Dist<DT, MT>::eval's.
-template <int DT, int MT, int C>
-struct DistRows {
-  static __device__ __forceinline__ void eval(const void* av, const uint8_t* const* rows,
-                                              const bool* act, uint32_t d, float* out) {
-    if (DT == DD_F32) {
-      const float* a = (const float*)av;
-      float r[C];
+// Distance from the query `q` (16-byte words, shared memory) to `row` computed
+// by a group of G lanes (G = 1, 2, 4 or 8, warp-uniform; `sub` = lane index in
+// the group).  Integer data: each lane sums the words sub, sub+G, ... and the
+// group adds the partial sums (exact integers, so any grouping gives the
+// reference's value).  Float data must keep the reference's summation order:
+// G must be 1 and the lane runs Dist::eval.  Every lane of the warp must call
+// it (the group reduction shuffles); lanes with act == false return 0.
+template <int DT, int MT>
+__device__ __forceinline__ float dist_group(const uint4* q, const uint8_t* row, uint32_t d,
+                                            uint32_t sub, uint32_t G, bool act) {
+  if (DT == DD_F32) return act ? Dist<DT, MT>::eval(q, row, d) : 0.f;
+  const uint32_t nv = (d + 15) >> 4;
+  const uint4* r4 = (const uint4*)row;
+  uint32_t acc = 0;
+  for (uint32_t w0 = sub; w0 < nv; w0 += 8 * G) {
+    uint4 y[8];
 #pragma unroll
-      for (int t = 0; t < C; t++) r[t] = 0.f;
-      uint32_t i = 0;
-      for (; i + 3 < d; i += 4) {
-        float4 x = *(const float4*)(a + i);
-        float4 y[C];
+    for (int i = 0; i < 8; i++) {
+      const uint32_t w = w0 + (uint32_t)i * G;
+      y[i] = (act && w < nv) ? __ldg(r4 + w) : make_uint4(0, 0, 0, 0);
+    }
 #pragma unroll
-        for (int t = 0; t < C; t++)
-          if (act[t]) y[t] = __ldg((const float4*)rows[t] + (i >> 2));
-#pragma unroll
-        for (int t = 0; t < C; t++) {
-          if (!act[t]) continue;
-          if (MT == DD_L2) {
-            float d0 = __fsub_rn(x.x, y[t].x), d1 = __fsub_rn(x.y, y[t].y);
-            float d2 = __fsub_rn(x.z, y[t].z), d3 = __fsub_rn(x.w, y[t].w);
-            float s = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)),
-                                          __fmul_rn(d2, d2)),
-                                __fmul_rn(d3, d3));
-            r[t] = __fadd_rn(r[t], s);
-          } else {
-            r[t] = __fadd_rn(r[t], __fmul_rn(x.x, y[t].x));
-            r[t] = __fadd_rn(r[t], __fmul_rn(x.y, y[t].y));
-            r[t] = __fadd_rn(r[t], __fmul_rn(x.z, y[t].z));
-            r[t] = __fadd_rn(r[t], __fmul_rn(x.w, y[t].w));
-          }
+    for (int i = 0; i < 8; i++) {
+      const uint32_t w = w0 + (uint32_t)i * G;
+      if (w < nv) {
+        const uint4 x = q[w];
+        if (MT == DD_L2) {
+          uint32_t s;
+          s = absdiff4<DT>(x.x, y[i].x); acc = __dp4a(s, s, acc);
+          s = absdiff4<DT>(x.y, y[i].y); acc = __dp4a(s, s, acc);
+          s = absdiff4<DT>(x.z, y[i].z); acc = __dp4a(s, s, acc);
+          s = absdiff4<DT>(x.w, y[i].w); acc = __dp4a(s, s, acc);
+        } else if (DT == DD_U8) {
+          acc = __dp4a(x.x, y[i].x, acc); acc = __dp4a(x.y, y[i].y, acc);
+          acc = __dp4a(x.z, y[i].z, acc); acc = __dp4a(x.w, y[i].w, acc);
+        } else {
+          int v = (int)acc;
+          v = __dp4a((int)x.x, (int)y[i].x, v); v = __dp4a((int)x.y, (int)y[i].y, v);
+          v = __dp4a((int)x.z, (int)y[i].z, v); v = __dp4a((int)x.w, (int)y[i].w, v);
+          acc = (uint32_t)v;
         }
       }
-      for (; i < d; i++) {
-#pragma unroll
-        for (int t = 0; t < C; t++) {
-          if (!act[t]) continue;
-          float yv = __ldg((const float*)rows[t] + i);
-          if (MT == DD_L2) {
-            float d0 = __fsub_rn(a[i], yv);
-            r[t] = __fadd_rn(r[t], __fmul_rn(d0, d0));
-          } else {
-            r[t] = __fadd_rn(r[t], __fmul_rn(a[i], yv));
-          }
-        }
-      }
-#pragma unroll
-      for (int t = 0; t < C; t++) out[t] = (MT == DD_L2) ? r[t] : -r[t];
-    } else {
-      const uint4* a = (const uint4*)av;
-      uint32_t nv = (d + 15) >> 4;
-      int acc[C];
-#pragma unroll
-      for (int t = 0; t < C; t++) acc[t] = 0;
-      for (uint32_t i = 0; i < nv; i++) {
-        uint4 x = a[i];
-        uint4 y[C];
-#pragma unroll
-        for (int t = 0; t < C; t++)
-          if (act[t]) y[t] = __ldg((const uint4*)rows[t] + i);
-#pragma unroll
-        for (int t = 0; t < C; t++) {
-          if (!act[t]) continue;
-          if (MT == DD_L2) {
-            uint32_t u = (uint32_t)acc[t], s;
-            s = absdiff4<DT>(x.x, y[t].x); u = __dp4a(s, s, u);
-            s = absdiff4<DT>(x.y, y[t].y); u = __dp4a(s, s, u);
-            s = absdiff4<DT>(x.z, y[t].z); u = __dp4a(s, s, u);
-            s = absdiff4<DT>(x.w, y[t].w); u = __dp4a(s, s, u);
-            acc[t] = (int)u;
-          } else if (DT == DD_U8) {
-            uint32_t u = (uint32_t)acc[t];
-            u = __dp4a(x.x, y[t].x, u); u = __dp4a(x.y, y[t].y, u);
-            u = __dp4a(x.z, y[t].z, u); u = __dp4a(x.w, y[t].w, u);
-            acc[t] = (int)u;
-          } else {
-            int v = acc[t];
-            v = __dp4a((int)x.x, (int)y[t].x, v); v = __dp4a((int)x.y, (int)y[t].y, v);
-            v = __dp4a((int)x.z, (int)y[t].z, v); v = __dp4a((int)x.w, (int)y[t].w, v);
-            acc[t] = v;
-          }
-        }
-      }
-#pragma unroll
-      for (int t = 0; t < C; t++)
-        out[t] = (MT == DD_L2) ? __int2float_rn(acc[t]) : -__int2float_rn(acc[t]);
     }
   }
-};
+  // wrap-around uint32 adds give the exact int32 total
+  for (uint32_t o = 1; o < G; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (!act) return 0.f;
+  return MT == DD_L2 ? __int2float_rn((int)acc) : -__int2float_rn((int)acc);
+}
 
 // splitmix64 finaliser: the reference's lossy "seen" filter hashes ids with it
 // (include/utils/beamSearch.h:66-73, include/parlay/utilities.h:145-150).

@@ -214,26 +214,37 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
       __syncwarp();
     }
 
-    // ---- distances of the kept neighbours (all chunks' loads interleaved)
-    float dist[CPL];
-    {
-      const uint8_t* rows[CPL];
-#pragma unroll
-      for (int t = 0; t < CPL; t++) rows[t] = P.points + (uint64_t)(keep[t] ? a[t] : 0) * P.stride;
-      DistRows<DT, MT, CPL>::eval(S.qv, rows, keep, P.d, dist);
-    }
-    uint32_t nc = 0;
+    // ---- the kept neighbours, compacted in neighbour order
+    uint32_t nk = 0;
 #pragma unroll
     for (int t = 0; t < CPL; t++) {
-      cmps += __popc(__ballot_sync(FULL, keep[t]));
-      bool pass = keep[t] && (dist[t] < cutoff);
-      uint32_t pb = __ballot_sync(FULL, pass);
-      if (pass) {
-        uint32_t pos = nc + __popc(pb & lanemask_lt());
-        S.c_id[pos] = a[t];
-        S.c_d[pos] = dist[t];
+      const uint32_t kb = __ballot_sync(FULL, keep[t]);
+      if (keep[t]) S.s_id[nk + __popc(kb & lanemask_lt())] = a[t];
+      nk += __popc(kb);
+    }
+    cmps += nk;
+    __syncwarp();
+    // ---- their distances: G lanes per neighbour for integer data (exact in
+    // any grouping), one lane for float data (the reference's summation order)
+    uint32_t nc = 0;
+    {
+      const uint32_t lg = (DT == DD_F32) ? 0u : (nk <= 8 ? 2u : (nk <= 16 ? 1u : 0u));
+      const uint32_t G = 1u << lg, per = 32u >> lg, sub = lane & (G - 1);
+      for (uint32_t k0 = 0; k0 < nk; k0 += per) {
+        const uint32_t k = k0 + (lane >> lg);
+        const bool act = k < nk;
+        const uint32_t id = act ? S.s_id[k] : 0u;
+        const float dist = dist_group<DT, MT>((const uint4*)S.qv, P.points + (uint64_t)id * P.stride,
+                                              P.d, sub, G, act);
+        const bool pass = act && sub == 0 && dist < cutoff;
+        const uint32_t pb = __ballot_sync(FULL, pass);
+        if (pass) {
+          const uint32_t pos = nc + __popc(pb & lanemask_lt());
+          S.c_id[pos] = id;
+          S.c_d[pos] = dist;
+        }
+        nc += __popc(pb);
       }
-      nc += __popc(pb);
     }
     __syncwarp();
     if (nc == 0) {
