@@ -54,8 +54,7 @@ WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, ui
     w.vis_id = w.vis_d = 0;  // global
     w.ws = off;
     // the selected rows of the register-row greedy share the prune workspace
-    const uint32_t nv = row_words16(d, dtype);
-    const uint32_t sel_bytes = nv <= reg_row_max_words(dtype) ? Rp * nv * 16u : 0u;
+    const uint32_t sel_bytes = greedy_sel_bytes(d, dtype, Rp);
     uint32_t pws = r16(4ull * w.ccap) * 2 + prune_ws_bytes_sel(w.ccap, sel_bytes);
     off += hash_bytes > pws ? hash_bytes : pws;
   } else {
@@ -177,12 +176,8 @@ __global__ void __launch_bounds__(64, 6) k_search_prune(IndexView ix, RoundArgs 
     }
     __syncwarp();
     warp_std_sort(W.Pm, m);
-    if (row_words16(ix.d, DT) <= (uint32_t)RegRow<DT>::NVM)
-      warp_greedy_select_reg<DT, MT>(ix.points, ix.stride, ix.d, p, W.Pm, m, ra.alpha, ix.R,
-                                     ra.new_out + b * ix.Rp, ix.Rp, W.Pm.sel);
-    else
-      warp_greedy_select<DT, MT>(ix.points, ix.stride, ix.d, p, W.Pm, m, ra.alpha, ix.R,
-                                 ra.new_out + b * ix.Rp, ix.Rp);
+    warp_greedy_select_fast<DT, MT>(ix.points, ix.stride, ix.d, p, W.Pm, m, ra.alpha, ix.R,
+                                    ra.new_out + b * ix.Rp, ix.Rp, W.Pm.sel);
     if (lane == 0) {
       if (ra.stat_vis) ra.stat_vis[b] = o.vis_n;
       if (ra.stat_cmps) ra.stat_cmps[b] = o.cmps;
@@ -209,8 +204,7 @@ __host__ __device__ inline RevLayout rev_layout(uint32_t d, int dtype, uint32_t 
   RevLayout r;
   uint32_t off = 0;
   uint32_t esz = dtype == DD_F32 ? 4 : 1;
-  const uint32_t nv = row_words16(d, dtype);
-  const uint32_t sel_bytes = nv <= reg_row_max_words(dtype) ? Rp * nv * 16u : 0u;
+  const uint32_t sel_bytes = greedy_sel_bytes(d, dtype, Rp);
   r.tv = off; off += r16((uint64_t)d * esz);
   r.cid = off; off += r16(4ull * kRevCandCap);
   r.ckey = off; off += r16(4ull * kRevCandCap);
@@ -256,11 +250,8 @@ __device__ void reverse_one(const IndexView& ix, const RoundArgs& ra, const Reve
   __syncwarp();
   const uint32_t m = s + deg;
   warp_std_sort(Pm, m);
-  if (row_words16(ix.d, DT) <= (uint32_t)RegRow<DT>::NVM)
-    warp_greedy_select_reg<DT, MT>(ix.points, ix.stride, ix.d, t, Pm, m, ra.alpha, ix.R, row,
-                                   ix.Rp, Pm.sel);
-  else
-    warp_greedy_select<DT, MT>(ix.points, ix.stride, ix.d, t, Pm, m, ra.alpha, ix.R, row, ix.Rp);
+  warp_greedy_select_fast<DT, MT>(ix.points, ix.stride, ix.d, t, Pm, m, ra.alpha, ix.R, row, ix.Rp,
+                                  Pm.sel);
   if (lane == 0) {
     atomicAdd(&rs.counters[2], 1u);
     atomicAdd(&rs.counters[3], m);
@@ -268,7 +259,7 @@ __device__ void reverse_one(const IndexView& ix, const RoundArgs& ra, const Reve
 }
 
 template <int DT, int MT>
-__global__ void __launch_bounds__(kRevWarps * 32, 4) k_reverse(IndexView ix, RoundArgs ra, ReverseScratch rs) {
+__global__ void __launch_bounds__(kRevWarps * 32, 7) k_reverse(IndexView ix, RoundArgs ra, ReverseScratch rs) {
   extern __shared__ uint4 smem_raw[];
   const RevLayout L = rev_layout(ix.d, DT, ix.Rp);
   const uint32_t wic = threadIdx.x >> 5, lane = lane_id();
@@ -800,10 +791,10 @@ void launch_reverse(const IndexView& ix, const RoundArgs& ra, const ReverseScrat
   if (!ra.B) return;
   RevLayout L = rev_layout(ix.d, ix.dtype, ix.Rp);
   size_t sm = (size_t)L.total * kRevWarps;
-  int rg = sm_count * 8;
 #define CALL(DT, MT)                                                                  \
   set_smem(k_reverse<DT, MT>, sm);                                                    \
-  k_reverse<DT, MT><<<rg, kRevWarps * 32, sm, st>>>(ix, ra, rs);                       \
+  k_reverse<DT, MT><<<sm_count * occupancy(k_reverse<DT, MT>, kRevWarps * 32, sm),     \
+                      kRevWarps * 32, sm, st>>>(ix, ra, rs);                          \
   k_reverse_big<DT, MT><<<kBigSlots, kBigThreads, 0, st>>>(ix, ra, rs);
   DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
 #undef CALL

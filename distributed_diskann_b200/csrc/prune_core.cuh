@@ -383,6 +383,278 @@ __device__ uint32_t warp_greedy_select_reg(const uint8_t* points, uint64_t strid
   return nsel;
 }
 
+// ---------------------------------------------------------------------------
+// Greedy selection on the tensor cores (integer data, rows of <= 128 bytes).
+//
+// The occlusion distances are exact integers, so they come from Gram tiles of
+// the rows: d(a, b) = |a|^2 + |b|^2 - 2 a.b for L2 and -a.b for MIPS, with a.b
+// from mma.sync m16n8k32 (u8 x u8 or s8 x s8, s32 accumulation: exact for
+// rows of <= 128 bytes), which is the reference's int32 value bit for bit.
+// The sorted list is walked in chunks of 16 candidates:
+//   1. the chunk's rows are staged in shared memory (right after the rows of
+//      the nsel already selected entries) with their squared norms;
+//   2. cross tiles (selected rows x chunk rows) remove every chunk member
+//      that some selected entry occludes;
+//   3. the chunk's own 16 x 16 tile gives, for each member j, the mask of
+//      members i < j with alpha * d(i, j) <= d(p, j); the chunk is then
+//      selected in order with bit operations, and the selected rows are
+//      compacted into the selected area.
+// Shared layout (`sel`): (Rp + 16) rows of 128 bytes, 16-byte words swizzled
+// by (row & 7) so the fragment loads are free of bank conflicts, then
+// (Rp + 16) norms, then 16 chunk occlusion thresholds.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kMmaChunk = 16;
+
+__host__ __device__ inline uint32_t mma_sel_bytes(uint32_t Rp) {
+  return (Rp + kMmaChunk) * 128u + (Rp + kMmaChunk) * 4u + kMmaChunk * 4u;
+}
+// the tensor-core form applies to integer data whose padded rows fit 128 bytes
+__host__ __device__ inline bool greedy_uses_mma(uint32_t d, int dtype) {
+  return dtype != DD_F32 && d <= 128;
+}
+// bytes the fast greedy forms need in the prune workspace (0: generic form)
+__host__ __device__ inline uint32_t greedy_sel_bytes(uint32_t d, int dtype, uint32_t Rp) {
+  if (greedy_uses_mma(d, dtype)) return mma_sel_bytes(Rp);
+  const uint32_t nv = row_words16(d, dtype);
+  return nv <= reg_row_max_words(dtype) ? Rp * nv * 16u : 0u;
+}
+
+template <int DT>
+__device__ __forceinline__ void mma_k32(int (&acc)[4], const uint32_t (&a)[4], uint32_t b0,
+                                        uint32_t b1) {
+  if (DT == DD_U8)
+    asm("mma.sync.aligned.m16n8k32.row.col.s32.u8.u8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};"
+        : "+r"(acc[0]), "+r"(acc[1]), "+r"(acc[2]), "+r"(acc[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+  else
+    asm("mma.sync.aligned.m16n8k32.row.col.s32.s8.s8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};"
+        : "+r"(acc[0]), "+r"(acc[1]), "+r"(acc[2]), "+r"(acc[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// 32-bit word q (0..31) of staged row r
+__device__ __forceinline__ uint32_t mma_row_word(const uint32_t* rw, uint32_t r, uint32_t q) {
+  return rw[r * 32u + (q ^ ((r & 7u) << 2))];
+}
+// 16-byte word w (0..7) of staged row r
+__device__ __forceinline__ uint4* mma_row_vec(uint32_t* rw, uint32_t r, uint32_t w) {
+  return (uint4*)(rw + r * 32u + ((w ^ (r & 7u)) << 2));
+}
+
+// acc[nt] += rows [ra0, ra0+16) x rows [rb0 + 8 nt, rb0 + 8 nt + 8), nt = 0, 1 (KS k-steps)
+template <int DT>
+__device__ __forceinline__ void mma_tile_16x16(const uint32_t* rw, uint32_t ra0, uint32_t rb0,
+                                               uint32_t KS, int (&acc)[2][4]) {
+  const uint32_t lane = lane_id(), g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+    for (int i = 0; i < 4; i++) acc[nt][i] = 0;
+  for (uint32_t ks = 0; ks < KS; ks++) {
+    const uint32_t q = 8 * ks + t;
+    uint32_t a[4];
+    a[0] = mma_row_word(rw, ra0 + g, q);
+    a[1] = mma_row_word(rw, ra0 + g + 8, q);
+    a[2] = mma_row_word(rw, ra0 + g, q + 4);
+    a[3] = mma_row_word(rw, ra0 + g + 8, q + 4);
+#pragma unroll
+    for (int nt = 0; nt < 2; nt++) {
+      const uint32_t rb = rb0 + 8 * nt + g;
+      mma_k32<DT>(acc[nt], a, mma_row_word(rw, rb, q), mma_row_word(rw, rb, q + 4));
+    }
+  }
+}
+
+// Largest integer x with alpha * (double)x <= key in the reference's double
+// arithmetic (alpha > 0).  Integer distances of rows <= 128 bytes have
+// |d| < 2^24, so the float the reference compares is the integer itself, and
+// the rounded product is monotone in x: "alpha * d <= key" is exactly
+// "d <= occlusion_threshold".  The result is clamped to +-2^25, which keeps
+// that equivalence for every |d| < 2^24; floor(key / alpha) is off by at most
+// one, so two correction steps each way suffice.
+__device__ __forceinline__ int occlusion_threshold(double alpha, float key) {
+  const double k = (double)key, lim = 33554432.0;
+  double x = floor(k / alpha);
+  x = fmin(fmax(x, -lim), lim);
+  for (int it = 0; it < 2 && x < lim && __dmul_rn(alpha, x + 1.0) <= k; it++) x += 1.0;
+  for (int it = 0; it < 2 && x > -lim && __dmul_rn(alpha, x) > k; it++) x -= 1.0;
+  return (int)x;
+}
+
+// the row-dependent part of a Gram distance: |a|^2 - 2 a.b (L2; the column's
+// |b|^2 is folded into its threshold) or -a.b (MIPS)
+template <int MT>
+__device__ __forceinline__ int gram_part(int na, int dot) {
+  return MT == DD_L2 ? na - 2 * dot : -dot;
+}
+
+// OR over the 8 rows of a ballot of fragment elements (lane = 4 g + t):
+// returns 4 bits, bit t set when some lane with that t voted
+__device__ __forceinline__ uint32_t any_over_rows(uint32_t b) {
+  b |= b >> 16;
+  b |= b >> 8;
+  b |= b >> 4;
+  return b & 0xFu;
+}
+// bits 0..3 -> bits 0, 2, 4, 6
+__device__ __forceinline__ uint32_t spread4(uint32_t x) {
+  return (x & 1u) | ((x & 2u) << 1) | ((x & 4u) << 2) | ((x & 8u) << 3);
+}
+// bits at positions 0, 4, ..., 28 -> bits 0..7
+__device__ __forceinline__ uint32_t gather_nibble_bits(uint32_t x) {
+  x &= 0x11111111u;
+  x = (x | (x >> 3)) & 0x03030303u;
+  x = (x | (x >> 6)) & 0x000F000Fu;
+  x = (x | (x >> 12)) & 0xFFu;
+  return x;
+}
+
+template <int DT, int MT>
+__device__ uint32_t warp_greedy_select_mma(const uint8_t* points, uint64_t stride, uint32_t d,
+                                           uint32_t p, const PruneSmem& S, uint32_t m,
+                                           double alpha, uint32_t R, uint32_t* out_row,
+                                           uint32_t Rp, uint4* sel) {
+  const uint32_t FULL = 0xffffffffu;
+  const uint32_t lane = lane_id(), g = lane >> 2, t = lane & 3;
+  uint32_t* rw = (uint32_t*)sel;
+  int* norms = (int*)(rw + (Rp + kMmaChunk) * 32u);
+  int* cthr = norms + Rp + kMmaChunk;
+  const uint32_t qb = (d + 15u) & ~15u;   // padded row bytes (integer data)
+  const uint32_t KS = (qb + 31u) >> 5;    // k-steps of 32 bytes
+  const uint32_t NW = 2u * KS;            // 16-byte words staged per row
+  uint32_t nsel = 0;
+  for (uint32_t c0 = 0; c0 < m && nsel < R; c0 += kMmaChunk) {
+    const uint32_t cnt = min(kMmaChunk, m - c0);
+    // ---- 1. stage the chunk: two lanes per member, rows nsel .. nsel + 15
+    uint32_t amask;
+    {
+      const uint32_t j = lane >> 1, h = lane & 1;
+      const uint32_t cj = j < cnt ? S.cid[c0 + j] : DD_NONE;
+      const bool alive = cj != DD_NONE && cj != p;
+      const uint32_t r = nsel + j;
+      const uint4* src = (const uint4*)(points + (uint64_t)(alive ? cj : 0u) * stride);
+      uint32_t nrm = 0;
+      for (uint32_t w = h; w < 8; w += 2) {
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (alive && w < NW) v = __ldg(src + w);
+        *mma_row_vec(rw, r, w) = v;
+        if (DT == DD_U8) {
+          nrm = __dp4a(v.x, v.x, nrm); nrm = __dp4a(v.y, v.y, nrm);
+          nrm = __dp4a(v.z, v.z, nrm); nrm = __dp4a(v.w, v.w, nrm);
+        } else {
+          int s = (int)nrm;
+          s = __dp4a((int)v.x, (int)v.x, s); s = __dp4a((int)v.y, (int)v.y, s);
+          s = __dp4a((int)v.z, (int)v.z, s); s = __dp4a((int)v.w, (int)v.w, s);
+          nrm = (uint32_t)s;
+        }
+      }
+      nrm += __shfl_xor_sync(FULL, nrm, 1);
+      if (h == 0) {
+        norms[r] = (int)nrm;
+        // occlusion of member j: L2 |a|^2 - 2 a.b <= T_j - |b|^2, MIPS -a.b <= T_j
+        const int T = alive ? occlusion_threshold(alpha, S.ckey[c0 + j]) : 0;
+        cthr[j] = MT == DD_L2 ? T - (int)nrm : T;
+      }
+      const bool a2 = __shfl_sync(FULL, alive ? 1 : 0, (2u * lane) & 31u) != 0;
+      amask = __ballot_sync(FULL, lane < kMmaChunk && a2);
+    }
+    __syncwarp();
+    // ---- 2. occlusion by the entries selected before this chunk
+    for (uint32_t r0 = 0; r0 < nsel && amask; r0 += 16) {
+      int acc[2][4];
+      mma_tile_16x16<DT>(rw, r0, nsel, KS, acc);
+      const uint32_t sa = r0 + g, sb = r0 + g + 8;
+      const int na = MT == DD_L2 ? norms[sa] : 0, nb = MT == DD_L2 ? norms[sb] : 0;
+      uint32_t occ = 0;
+#pragma unroll
+      for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int thr = cthr[8u * nt + 2u * t + e];
+          const bool oa = sa < nsel && gram_part<MT>(na, acc[nt][e]) <= thr;
+          const bool ob = sb < nsel && gram_part<MT>(nb, acc[nt][2 + e]) <= thr;
+          occ |= spread4(any_over_rows(__ballot_sync(FULL, oa || ob))) << (8 * nt + e);
+        }
+      amask &= ~occ;
+    }
+    // ---- 3. the chunk's own tile, then in-order selection with bit masks
+    uint32_t colmask[kMmaChunk];
+    {
+      int acc[2][4];
+      mma_tile_16x16<DT>(rw, nsel, nsel, KS, acc);
+      const int na = MT == DD_L2 ? norms[nsel + g] : 0;
+      const int nb = MT == DD_L2 ? norms[nsel + g + 8] : 0;
+#pragma unroll
+      for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const uint32_t col = 8u * nt + 2u * t + e;
+          const int thr = cthr[col];
+          const bool oa = g < col && gram_part<MT>(na, acc[nt][e]) <= thr;
+          const bool ob = g + 8 < col && gram_part<MT>(nb, acc[nt][2 + e]) <= thr;
+          const uint32_t bl = __ballot_sync(FULL, oa), bh = __ballot_sync(FULL, ob);
+#pragma unroll
+          for (int tt = 0; tt < 4; tt++)
+            colmask[8 * nt + 2 * tt + e] =
+                gather_nibble_bits(bl >> tt) | (gather_nibble_bits(bh >> tt) << 8);
+        }
+    }
+    uint32_t selm = 0, ns = nsel;
+#pragma unroll
+    for (int j = 0; j < (int)kMmaChunk; j++)
+      if (ns < R && ((amask >> j) & 1u) && (colmask[j] & selm) == 0) {
+        selm |= 1u << j;
+        ns++;
+      }
+    // ---- output ids in order; compact the selected rows (read all, then write)
+    {
+      const uint32_t j = lane >> 1, h = lane & 1;
+      const bool s = (selm >> j) & 1u;
+      const uint32_t k = __popc(selm & ((1u << j) - 1u));
+      if (s && h == 0) out_row[nsel + k] = S.cid[c0 + j];
+      uint4 v[4];
+      int nrm = 0;
+      if (s) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) v[i] = *mma_row_vec(rw, nsel + j, 2u * i + h);
+        nrm = norms[nsel + j];
+      }
+      __syncwarp();
+      if (s) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) *mma_row_vec(rw, nsel + k, 2u * i + h) = v[i];
+        if (h == 0) norms[nsel + k] = nrm;
+      }
+      __syncwarp();
+    }
+    nsel = ns;
+  }
+  for (uint32_t j = nsel + lane; j < Rp; j += 32) out_row[j] = DD_NONE;
+  __syncwarp();
+  return nsel;
+}
+
+// The fastest exact greedy form for the data type; `sel` holds
+// greedy_sel_bytes(d, DT, Rp) bytes (unused by the generic form).
+template <int DT, int MT>
+__device__ __forceinline__ uint32_t warp_greedy_select_fast(const uint8_t* points, uint64_t stride,
+                                                            uint32_t d, uint32_t p,
+                                                            const PruneSmem& S, uint32_t m,
+                                                            double alpha, uint32_t R,
+                                                            uint32_t* out_row, uint32_t Rp,
+                                                            uint4* sel) {
+  if (DT != DD_F32) {
+    if (greedy_uses_mma(d, DT))
+      return warp_greedy_select_mma<DT, MT>(points, stride, d, p, S, m, alpha, R, out_row, Rp,
+                                            sel);
+  } else if (row_words16(d, DT) <= (uint32_t)RegRow<DT>::NVM) {
+    return warp_greedy_select_reg<DT, MT>(points, stride, d, p, S, m, alpha, R, out_row, Rp, sel);
+  }
+  return warp_greedy_select<DT, MT>(points, stride, d, p, S, m, alpha, R, out_row, Rp);
+}
+
 // byte offset of the (16-byte aligned) selected-row area inside a prune
 // workspace of `cap` candidates: it overlays the rank-pairing scratch, which
 // is dead once the sort is done
