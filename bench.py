@@ -361,7 +361,7 @@ def main():
             "clocks": clk,
             "build_stats": {k2: st[k2] for k2 in ("rounds", "visited", "dist_cmps", "groups",
                                                  "reverse_prunes", "prune_cands", "big_groups",
-                                                 "build_ms", "search_prune_ms", "reverse_ms")},
+                                                 "build_ms", "search_prune_ms", "search_ms", "reverse_ms")},
             "graph": {"avg_degree": float(deg.mean()), "max_degree": int(deg.max())},
             "queries": qres,
             "setup_s": {"datagen": gen_s},

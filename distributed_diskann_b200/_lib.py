@@ -34,7 +34,8 @@ class BuildParamsC(C.Structure):
 class StatsC(C.Structure):
     _fields_ = [("rounds", u64), ("visited", u64), ("dist_cmps", u64), ("groups", u64),
                 ("reverse_prunes", u64), ("prune_cands", u64), ("big_groups", u64),
-                ("build_ms", dbl), ("search_prune_ms", dbl), ("reverse_ms", dbl)]
+                ("build_ms", dbl), ("search_prune_ms", dbl), ("reverse_ms", dbl),
+                ("search_ms", dbl)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -51,15 +51,13 @@ struct dd_index {
   uint32_t* gbits = nullptr;
   int* granges = nullptr;
   uint64_t gcap = 0;
-  // per-warp visited-list slices of the build searches (grown on demand)
-  uint32_t* hash_arena = nullptr;
-  uint64_t hash_arena_words = 0;
+  // per-point visited-list slices of the build searches (grown on demand)
+  uint32_t* vis_all = nullptr;
+  uint64_t vis_all_words = 0;
   bool verbose = false;
 };
 
 namespace {
-
-constexpr int kSearchWarpsPerCta = 2;
 
 int fail(dd_index* h, int code, const char* fmt, ...) {
   char buf[512];
@@ -197,16 +195,19 @@ SemisortScratch make_ss(dd_index* h) {
   return s;
 }
 
-// room for `words` uint32 of per-warp hash tables
-int ensure_hash_arena(dd_index* h, uint64_t words) {
-  if (words <= h->hash_arena_words) return DD_OK;
-  dfree(h->hash_arena);
-  h->hash_arena = nullptr;
-  h->hash_arena_words = 0;
-  CK(dalloc(&h->hash_arena, words));
-  h->hash_arena_words = words;
+// room for `words` uint32 of per-point visited lists
+int ensure_vis_all(dd_index* h, uint64_t words) {
+  if (words <= h->vis_all_words) return DD_OK;
+  dfree(h->vis_all);
+  h->vis_all = nullptr;
+  h->vis_all_words = 0;
+  CK(dalloc(&h->vis_all, words));
+  h->vis_all_words = words;
   return DD_OK;
 }
+
+// ids fit the 24-bit hash table layout
+bool use_h24(const dd_index* h) { return h->n < 0xFFFFFFull; }
 
 // the reverse-edge scratch of a handle; `res` = semisort result buffer
 ReverseScratch make_rs(dd_index* h, int res) {
@@ -261,13 +262,16 @@ struct PhaseEvents {
     }
     return ev[used++];
   }
-  void sum(float* t_search, float* t_rev) {
-    for (size_t i = 0; i + 2 < used; i += 3) {
-      float a = 0, b = 0;
+  // events per round: start | search done | prune done | reverse done
+  void sum(float* t_search, float* t_prune, float* t_rev) {
+    for (size_t i = 0; i + 3 < used; i += 4) {
+      float a = 0, b = 0, c = 0;
       cudaEventElapsedTime(&a, ev[i], ev[i + 1]);
       cudaEventElapsedTime(&b, ev[i + 1], ev[i + 2]);
+      cudaEventElapsedTime(&c, ev[i + 2], ev[i + 3]);
       *t_search += a;
-      *t_rev += b;
+      *t_prune += b;
+      *t_rev += c;
     }
   }
   ~PhaseEvents() {
@@ -275,8 +279,16 @@ struct PhaseEvents {
   }
 };
 
+// The launch shapes of one build: search and prune layouts and CTA plans.
+struct BuildPlan {
+  WarpLayout slay;
+  LaunchPlan splan;
+  PruneLayout play;
+  LaunchPlan pplan;
+};
+
 int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& rounds, double alpha,
-                const dd_build_params* P, const WarpLayout& lay, int grid_max, PhaseEvents* pe) {
+                const dd_build_params* P, const BuildPlan& bp, PhaseEvents* pe) {
   IndexView ix = view(h);
   for (auto& rd : rounds) {
     uint64_t B = rd.second > rd.first ? rd.second - rd.first : 0;
@@ -290,18 +302,28 @@ int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& r
     ra.new_out = h->new_out;
     ra.stat_vis = h->stat_vis;
     ra.stat_cmps = h->stat_cmps;
-    ra.vis_arena = h->hash_arena;
+    ra.vis_all = h->vis_all;
     CK(cudaMemsetAsync(h->counters, 0, 8 * 4, h->stream));
     if (pe) CK(cudaEventRecord(pe->next(), h->stream));
-    int grid = (int)std::min<uint64_t>((B + kSearchWarpsPerCta - 1) / kSearchWarpsPerCta,
-                                       (uint64_t)grid_max);
-    launch_search_prune(ix, ra, lay, kSearchWarpsPerCta, grid, h->stream);
+    {
+      const uint64_t wpc = (uint64_t)bp.splan.warps_per_cta;
+      const int grid = (int)std::min<uint64_t>(
+          (B + wpc - 1) / wpc, (uint64_t)bp.splan.blocks_per_sm * h->sm_count);
+      launch_search(ix, ra, bp.slay, bp.splan, grid, h->stream);
+    }
+    if (pe) CK(cudaEventRecord(pe->next(), h->stream));
+    {
+      const uint64_t wpc = (uint64_t)bp.pplan.warps_per_cta;
+      const int grid = (int)std::min<uint64_t>(
+          (B + wpc - 1) / wpc, (uint64_t)bp.pplan.blocks_per_sm * h->sm_count);
+      launch_prune_round(ix, ra, bp.play, bp.slay.vcap, bp.pplan, grid, h->stream);
+    }
     if (pe) CK(cudaEventRecord(pe->next(), h->stream));
     launch_apply_rows(ix, ra, h->stream);
     SemisortScratch ss = make_ss(h);
     const int res = launch_semisort(h->new_out, B * h->Rp, h->n, ss, h->stream);
     launch_reverse(ix, ra, make_rs(h, res), h->stream, h->sm_count);
-    h->launches += 6 + 5 * (uint64_t)((64 - __builtin_clzll(h->n > 1 ? h->n - 1 : 1) + 7) / 8);
+    h->launches += 7 + 5 * (uint64_t)((64 - __builtin_clzll(h->n > 1 ? h->n - 1 : 1) + 7) / 8);
     if (P->collect_stats) {
       k_accumulate<<<64, 256, 0, h->stream>>>(h->stat_vis, h->stat_cmps, (uint32_t)B, h->counters,
                                               h->acc);
@@ -373,7 +395,7 @@ int dd_destroy(dd_index* h) {
   void* ptrs[] = {h->points, h->graph, h->err, h->new_out, h->stat_vis, h->stat_cmps,
                   h->sort_t[0], h->sort_t[1], h->sort_v[0], h->sort_v[1], h->hist, h->heads,
                   h->flags, h->counters, h->big, h->block_sums, h->acc, h->gcand, h->gkey,
-                  h->gpos, h->gbits, h->granges, h->hash_arena};
+                  h->gpos, h->gbits, h->granges, h->vis_all};
   for (void* p : ptrs) dfree(p);
   delete h;
   return DD_OK;
@@ -518,12 +540,18 @@ int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
   int rc = ensure_build_scratch(h, Bmax);
   if (rc) return rc;
   uint32_t vcap = P->vcap ? P->vcap : 4 * P->L;
-  WarpLayout lay = make_search_layout(h->d, h->dtype, P->L, h->Rp, vcap, true);
-  if ((size_t)lay.total * kSearchWarpsPerCta > 227 * 1024)
-    return fail(h, DD_ERR_UNSUPPORTED, "per-warp shared memory %u B too large (L=%u)", lay.total, P->L);
-  const int bps = search_blocks_per_sm(view(h), lay, P->L, kSearchWarpsPerCta, true);
-  const int grid_max = bps * h->sm_count;
-  rc = ensure_hash_arena(h, (uint64_t)grid_max * kSearchWarpsPerCta * 2ull * lay.vcap);
+  BuildPlan bp;
+  bp.slay = make_search_layout(h->d, h->dtype, P->L, h->Rp, vcap, true, use_h24(h));
+  if (bp.slay.total > 227 * 1024)
+    return fail(h, DD_ERR_UNSUPPORTED, "per-warp shared memory %u B too large (L=%u)",
+                bp.slay.total, P->L);
+  bp.play = make_prune_layout(h->d, h->dtype, h->Rp, bp.slay.ccap);
+  if (bp.play.total > 227 * 1024)
+    return fail(h, DD_ERR_UNSUPPORTED, "prune shared memory %u B too large (visited capacity %u)",
+                bp.play.total, vcap);
+  bp.splan = plan_search(view(h), bp.slay, P->L);
+  bp.pplan = plan_prune(view(h), bp.play);
+  rc = ensure_vis_all(h, Bmax * 2ull * vcap);
   if (rc) return rc;
 
   // empty graph (the reference starts from Graph(R, n): all degrees 0)
@@ -536,14 +564,14 @@ int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
   PhaseEvents pe;
   PhaseEvents* pep = stats ? &pe : nullptr;
   CK(cudaEventRecord(e0, h->stream));
-  float ts = 0, tr = 0;
+  float ts = 0, tp = 0, tr = 0;
   dd_build_params Q = *P;
   Q.start_point = start;
   if (P->two_pass) {
-    rc = pass_rounds(h, rounds, 1.0, &Q, lay, grid_max, pep);
+    rc = pass_rounds(h, rounds, 1.0, &Q, bp, pep);
     if (rc) return rc;
   }
-  rc = pass_rounds(h, rounds, P->alpha, &Q, lay, grid_max, pep);
+  rc = pass_rounds(h, rounds, P->alpha, &Q, bp, pep);
   if (rc) return rc;
   if (P->knn_mode) {
     launch_sort_rows(view(h), h->stream);
@@ -556,7 +584,7 @@ int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
   if (stats) {
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
-    pe.sum(&ts, &tr);
+    pe.sum(&ts, &tp, &tr);
     unsigned long long acc[8] = {0};
     cudaMemcpy(acc, h->acc, sizeof acc, cudaMemcpyDeviceToHost);
     std::memset(stats, 0, sizeof *stats);
@@ -568,8 +596,9 @@ int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
     stats->prune_cands = acc[4];
     stats->big_groups = acc[5];
     stats->build_ms = ms;
-    stats->search_prune_ms = ts;
+    stats->search_prune_ms = ts + tp;
     stats->reverse_ms = tr;
+    stats->search_ms = ts;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -588,12 +617,12 @@ int dd_search_device(dd_index* h, const void* queries, uint64_t nq, uint64_t qst
   if (qstride % 16) return fail(h, DD_ERR_ARG, "device query stride must be a multiple of 16");
   CK(cudaSetDevice(h->device));
   h->launches = 0;
-  WarpLayout lay = make_search_layout(h->d, h->dtype, Lmax, h->Rp, 2 * Lmax + 64, false);
+  WarpLayout lay = make_search_layout(h->d, h->dtype, Lmax, h->Rp, 2 * Lmax + 64, false, use_h24(h));
   int wpc = 4;
   while (wpc > 1 && (size_t)lay.total * wpc > 227 * 1024) wpc >>= 1;
   if ((size_t)lay.total * wpc > 227 * 1024)
     return fail(h, DD_ERR_UNSUPPORTED, "query shared memory %u B too large", lay.total);
-  const int bps = search_blocks_per_sm(view(h), lay, Lmax, wpc, false);
+  const int bps = search_blocks_per_sm(view(h), lay, Lmax, wpc);
   const int grid = (int)std::min<uint64_t>((nq + wpc - 1) / wpc, (uint64_t)bps * h->sm_count);
   QueryArgs qa;
   qa.queries = (const uint8_t*)queries;
@@ -669,7 +698,7 @@ int dd_beam_search(dd_index* h, const void* queries, uint64_t nq, uint64_t qstri
   if (start >= h->n) return fail(h, DD_ERR_ARG, "start point >= n");
   CK(cudaSetDevice(h->device));
   uint64_t rb = (uint64_t)h->d * esize(h->dtype), ds = h->stride;
-  WarpLayout lay = make_search_layout(h->d, h->dtype, L, h->Rp, vcap, false);
+  WarpLayout lay = make_search_layout(h->d, h->dtype, L, h->Rp, vcap, false, use_h24(h));
   if (lay.total > 227 * 1024) return fail(h, DD_ERR_UNSUPPORTED, "beam shared memory too large");
   const int bgrid = (int)std::min<uint64_t>(nq, 4096);
   uint8_t* dq = nullptr;

@@ -1,8 +1,11 @@
 // Device kernels of the B200 Vamana hot path.
 //
-//   k_search_prune : one warp per batch point: beam_search on the round-start
-//                    graph, then robustPrune of the visited list
-//                    (include/index.h:274-285; src/bsp_index.hpp:259-277)
+//   k_search       : one warp per batch point: beam_search on the round-start
+//                    graph; the visited list goes to the point's global slice
+//                    (include/index.h:274-278; src/bsp_index.hpp:259-268)
+//   k_prune        : one warp per batch point: robustPrune of the visited list
+//                    and the point's out-list (include/index.h:279-285;
+//                    src/bsp_index.hpp:269-277)
 //   k_apply_rows   : update_neighbors of the batch (src/bsp_index.hpp:354-357)
 //   k_emit_count / scan / k_scatter : flatten (target, source) pairs and group
 //                    them by target keeping batch order inside a target
@@ -28,14 +31,14 @@ static __host__ __device__ inline uint32_t r16(uint64_t x) {
   return (uint32_t)((x + 15) & ~(uint64_t)15);
 }
 
-// Per-warp shared memory:
-//   build (with_prune): qv | frontier | step candidates | hash table, where the
-//     hash region is reused after the search as the prune workspace (visited
-//     list + out-list candidates, leaf bitmap, stack); the visited list is
-//     appended to a per-warp global slice during the search.
-//   query / debug: qv | frontier | step candidates | visited (debug) | evicted | hash.
+// Per-warp shared memory of the search kernels:
+//   build search: qv | frontier | step candidates | hash table; the visited
+//     list goes to the point's slice of a global array (read by k_prune).
+//   query / debug: qv | frontier | step candidates | visited | evicted | hash.
+// With h24 the hash table stores 24-bit ids (3 bytes a slot instead of 4),
+// which is exact whenever every id is below 0xFFFFFF.
 WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, uint32_t vcap,
-                              bool with_prune) {
+                              bool build, bool h24) {
   WarpLayout w{};
   uint32_t esz = dtype == DD_F32 ? 4 : 1;
   uint32_t off = 0;
@@ -49,14 +52,12 @@ WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, ui
   w.vcap = vcap;
   w.ccap = vcap + Rp;
   w.hbits = hash_bits_for(L);
-  const uint32_t hash_bytes = 4u << w.hbits;
-  if (with_prune) {
+  w.h24 = h24 ? 1u : 0u;
+  const uint32_t hash_bytes = r16(hash_table_bytes(w.hbits, h24));
+  if (build) {
     w.vis_id = w.vis_d = 0;  // global
     w.ws = off;
-    // the selected rows of the register-row greedy share the prune workspace
-    const uint32_t sel_bytes = greedy_sel_bytes(d, dtype, Rp);
-    uint32_t pws = r16(4ull * w.ccap) * 2 + prune_ws_bytes_sel(w.ccap, sel_bytes);
-    off += hash_bytes > pws ? hash_bytes : pws;
+    off += hash_bytes;
   } else {
     w.vis_id = off; off += r16(4ull * vcap);
     w.vis_d = off; off += r16(4ull * vcap);
@@ -67,49 +68,55 @@ WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, ui
   return w;
 }
 
-struct WarpPtrs {
-  SearchSmem S;
-  PruneSmem Pm;
-};
+// Per-warp shared memory of k_prune: p's vector | candidate ids | distances |
+// sort workspace, which the fast greedy forms share after the sort.
+PruneLayout make_prune_layout(uint32_t d, int dtype, uint32_t Rp, uint32_t ccap) {
+  PruneLayout w{};
+  uint32_t esz = dtype == DD_F32 ? 4 : 1;
+  uint32_t off = 0;
+  w.qv = off; off += r16((uint64_t)d * esz);
+  w.cid = off; off += r16(4ull * ccap);
+  w.ckey = off; off += r16(4ull * ccap);
+  w.ws = off; off += prune_ws_bytes_sel(ccap, greedy_sel_bytes(d, dtype, Rp));
+  w.ccap = ccap;
+  w.total = r16(off);
+  return w;
+}
 
-// build layout: visited list in the global slice vis_g (vcap ids then vcap dists)
-__device__ __forceinline__ WarpPtrs carve_build(uint8_t* base, const WarpLayout& w, uint32_t* vis_g) {
-  WarpPtrs r;
-  r.S.qv = base + w.qv;
-  r.S.fr_id = (uint32_t*)(base + w.fr_id);
-  r.S.fr_d = (float*)(base + w.fr_d);
-  r.S.c_id = (uint32_t*)(base + w.c_id);
-  r.S.c_d = (float*)(base + w.c_d);
-  r.S.s_id = (uint32_t*)(base + w.s_id);
-  r.S.s_d = (float*)(base + w.s_d);
-  r.S.vis_id = vis_g;
-  r.S.vis_d = (float*)(vis_g + w.vcap);
-  r.S.ev_id = nullptr;
-  r.S.hash = (uint32_t*)(base + w.ws);
-  // after the search the hash region holds the prune workspace
-  uint8_t* ws = base + w.ws;
-  const uint32_t cb = r16(4ull * w.ccap);
-  r.Pm = prune_ws((uint32_t*)ws, (float*)(ws + cb), ws + 2 * cb, w.ccap);
-  r.Pm.sel = (uint4*)(ws + 2 * cb + prune_sel_offset(w.ccap));
-  return r;
+// build search: visited list in the global slice vis_g (vcap ids then vcap dists)
+__device__ __forceinline__ SearchSmem carve_build(uint8_t* base, const WarpLayout& w, uint32_t* vis_g) {
+  SearchSmem S;
+  S.qv = base + w.qv;
+  S.fr_id = (uint32_t*)(base + w.fr_id);
+  S.fr_d = (float*)(base + w.fr_d);
+  S.c_id = (uint32_t*)(base + w.c_id);
+  S.c_d = (float*)(base + w.c_d);
+  S.s_id = (uint32_t*)(base + w.s_id);
+  S.s_d = (float*)(base + w.s_d);
+  S.vis_id = vis_g;
+  S.vis_d = (float*)(vis_g + w.vcap);
+  S.ev_id = nullptr;
+  S.hash = (uint32_t*)(base + w.ws);
+  S.h24 = (int)w.h24;
+  return S;
 }
 
 // query / debug layout: everything in shared memory
-__device__ __forceinline__ WarpPtrs carve_query(uint8_t* base, const WarpLayout& w) {
-  WarpPtrs r;
-  r.S.qv = base + w.qv;
-  r.S.fr_id = (uint32_t*)(base + w.fr_id);
-  r.S.fr_d = (float*)(base + w.fr_d);
-  r.S.c_id = (uint32_t*)(base + w.c_id);
-  r.S.c_d = (float*)(base + w.c_d);
-  r.S.s_id = (uint32_t*)(base + w.s_id);
-  r.S.s_d = (float*)(base + w.s_d);
-  r.S.vis_id = (uint32_t*)(base + w.vis_id);
-  r.S.vis_d = (float*)(base + w.vis_d);
-  r.S.ev_id = (uint32_t*)(base + w.ws);
-  r.S.hash = (uint32_t*)(base + w.ws + r16(4ull * w.vcap));
-  r.Pm = PruneSmem{};
-  return r;
+__device__ __forceinline__ SearchSmem carve_query(uint8_t* base, const WarpLayout& w) {
+  SearchSmem S;
+  S.qv = base + w.qv;
+  S.fr_id = (uint32_t*)(base + w.fr_id);
+  S.fr_d = (float*)(base + w.fr_d);
+  S.c_id = (uint32_t*)(base + w.c_id);
+  S.c_d = (float*)(base + w.c_d);
+  S.s_id = (uint32_t*)(base + w.s_id);
+  S.s_d = (float*)(base + w.s_d);
+  S.vis_id = (uint32_t*)(base + w.vis_id);
+  S.vis_d = (float*)(base + w.vis_d);
+  S.ev_id = (uint32_t*)(base + w.ws);
+  S.hash = (uint32_t*)(base + w.ws + r16(4ull * w.vcap));
+  S.h24 = (int)w.h24;
+  return S;
 }
 
 // copy a padded vector row into shared memory (16-byte granules)
@@ -131,15 +138,16 @@ __device__ __forceinline__ uint32_t row_degree(const uint32_t* row, uint32_t Rp)
 }
 
 // ============================================================ build round
+// k_search: one warp per batch point runs beam_search on the round-start graph
+// and leaves its visited list in the point's global slice
+// (include/index.h:274-278; src/bsp_index.hpp:259-268).
 template <int DT, int MT, int FPL, int CPL>
-__global__ void __launch_bounds__(64, 6) k_search_prune(IndexView ix, RoundArgs ra, WarpLayout lay) {
+__global__ void __launch_bounds__(512) k_search(IndexView ix, RoundArgs ra, WarpLayout lay) {
   extern __shared__ uint4 smem_raw[];
   const uint32_t wpc = blockDim.x >> 5;
   const uint32_t wic = threadIdx.x >> 5;
-  const uint32_t lane = lane_id();
   const uint64_t gw = (uint64_t)blockIdx.x * wpc + wic;
-  WarpPtrs W = carve_build((uint8_t*)smem_raw + (size_t)wic * lay.total, lay,
-                           ra.vis_arena + gw * 2ull * lay.vcap);
+  uint8_t* base = (uint8_t*)smem_raw + (size_t)wic * lay.total;
   SearchParams P;
   P.points = ix.points; P.stride = ix.stride; P.graph = ix.graph; P.Rp = ix.Rp; P.n = ix.n;
   P.d = ix.d; P.start = ra.start; P.L = ra.L; P.k = 0; P.cut = 0.0; P.limit = ix.n;
@@ -148,41 +156,64 @@ __global__ void __launch_bounds__(64, 6) k_search_prune(IndexView ix, RoundArgs 
   const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
   for (uint64_t b = gw; b < ra.B; b += (uint64_t)gridDim.x * wpc) {
     const uint32_t p = (uint32_t)(ra.floor + b);
-    load_vec(W.S.qv, ix.points + (uint64_t)p * ix.stride, qb);
+    const SearchSmem S = carve_build(base, lay, ra.vis_all + b * 2ull * lay.vcap);
+    load_vec(S.qv, ix.points + (uint64_t)p * ix.stride, qb);
     __syncwarp();
-    SearchOut o = warp_beam_search<DT, MT, FPL, CPL>(P, W.S, p);
-    uint32_t m = o.vis_n;
-    // the visited list moves into the (now free) hash region, sorted by
-    // (dist, id) like the reference's
-    for (uint32_t j = lane; j < m; j += 32) {
-      W.Pm.cid[j] = W.S.vis_id[j];
-      W.Pm.ckey[j] = W.S.vis_d[j];
+    const SearchOut o = warp_beam_search<DT, MT, FPL, CPL>(P, S, p);
+    if (lane_id() == 0) {
+      ra.stat_vis[b] = o.vis_n;
+      if (ra.stat_cmps) ra.stat_cmps[b] = o.cmps;
     }
     __syncwarp();
-    warp_sort_pairs(W.Pm.cid, W.Pm.ckey, m);
+  }
+}
+
+// k_prune: one warp per batch point runs robustPrune of its visited list plus
+// its current out-list (include/index.h:279-285; src/bsp_index.hpp:269-277).
+template <int DT, int MT>
+__global__ void __launch_bounds__(512) k_prune(IndexView ix, RoundArgs ra, PruneLayout lay,
+                                               uint32_t vcap) {
+  extern __shared__ uint4 smem_raw[];
+  const uint32_t wpc = blockDim.x >> 5;
+  const uint32_t wic = threadIdx.x >> 5;
+  const uint32_t lane = lane_id();
+  const uint64_t gw = (uint64_t)blockIdx.x * wpc + wic;
+  uint8_t* base = (uint8_t*)smem_raw + (size_t)wic * lay.total;
+  uint8_t* qv = base + lay.qv;
+  PruneSmem Pm = prune_ws((uint32_t*)(base + lay.cid), (float*)(base + lay.ckey), base + lay.ws,
+                          lay.ccap);
+  Pm.sel = (uint4*)(base + lay.ws + prune_sel_offset(lay.ccap));
+  const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
+  for (uint64_t b = gw; b < ra.B; b += (uint64_t)gridDim.x * wpc) {
+    const uint32_t p = (uint32_t)(ra.floor + b);
+    load_vec(qv, ix.points + (uint64_t)p * ix.stride, qb);
+    // the visited list, sorted by (dist, id) like the reference's
+    const uint32_t* vis = ra.vis_all + b * 2ull * vcap;
+    uint32_t m = min(ra.stat_vis[b], vcap);
+    for (uint32_t j = lane; j < m; j += 32) {
+      Pm.cid[j] = vis[j];
+      Pm.ckey[j] = __uint_as_float(vis[vcap + j]);
+    }
+    __syncwarp();
+    warp_sort_pairs(Pm.cid, Pm.ckey, m);
     // robustPrune adds p's current out-list (round-start snapshot)
     const uint32_t* prow = ix.graph + (uint64_t)p * ix.Rp;
-    for (uint32_t base = 0; base < ix.Rp; base += 32) {
-      uint32_t j = base + lane;
-      uint32_t a = (j < ix.Rp) ? prow[j] : DD_NONE;
-      bool v = a != DD_NONE;
-      uint32_t vb = __ballot_sync(0xffffffffu, v);
+    for (uint32_t b0 = 0; b0 < ix.Rp; b0 += 32) {
+      const uint32_t j = b0 + lane;
+      const uint32_t a = (j < ix.Rp) ? prow[j] : DD_NONE;
+      const bool v = a != DD_NONE;
+      const uint32_t vb = __ballot_sync(0xffffffffu, v);
       if (v) {
-        uint32_t pos = m + __popc(vb & lanemask_lt());
-        W.Pm.cid[pos] = a;
-        W.Pm.ckey[pos] = Dist<DT, MT>::eval(W.S.qv, ix.points + (uint64_t)a * ix.stride, ix.d);
+        const uint32_t pos = m + __popc(vb & lanemask_lt());
+        Pm.cid[pos] = a;
+        Pm.ckey[pos] = Dist<DT, MT>::eval(qv, ix.points + (uint64_t)a * ix.stride, ix.d);
       }
       m += __popc(vb);
     }
     __syncwarp();
-    warp_std_sort(W.Pm, m);
-    warp_greedy_select_fast<DT, MT>(ix.points, ix.stride, ix.d, p, W.Pm, m, ra.alpha, ix.R,
-                                    ra.new_out + b * ix.Rp, ix.Rp, W.Pm.sel);
-    if (lane == 0) {
-      if (ra.stat_vis) ra.stat_vis[b] = o.vis_n;
-      if (ra.stat_cmps) ra.stat_cmps[b] = o.cmps;
-    }
-    __syncwarp();
+    warp_std_sort(Pm, m);
+    warp_greedy_select_fast<DT, MT>(ix.points, ix.stride, ix.d, p, Pm, m, ra.alpha, ix.R,
+                                    ra.new_out + b * ix.Rp, ix.Rp, Pm.sel);
   }
 }
 
@@ -454,7 +485,7 @@ __global__ void __launch_bounds__(128) k_query(IndexView ix, QueryArgs qa, WarpL
   extern __shared__ uint4 smem_raw[];
   const uint32_t wpc = blockDim.x >> 5, wic = threadIdx.x >> 5, lane = lane_id();
   const uint64_t gw = (uint64_t)blockIdx.x * wpc + wic;
-  WarpPtrs W = carve_query((uint8_t*)smem_raw + (size_t)wic * lay.total, lay);
+  const SearchSmem S = carve_query((uint8_t*)smem_raw + (size_t)wic * lay.total, lay);
   const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
   for (uint64_t q = gw; q < qa.nq; q += (uint64_t)gridDim.x * wpc) {
     SearchParams P;
@@ -467,13 +498,13 @@ __global__ void __launch_bounds__(128) k_query(IndexView ix, QueryArgs qa, WarpL
     P.d = ix.d; P.start = qa.start; P.L = Lq; P.k = qa.k; P.cut = qa.cut; P.limit = qa.limit;
     P.degree_limit = qa.degree_limit; P.hbits = hash_bits_for(P.L); P.vcap = lay.vcap;
     P.query_mode = 1; P.keep_visited = 0; P.err = ix.err;
-    load_vec(W.S.qv, qa.queries + q * qa.qstride, qb);
+    load_vec(S.qv, qa.queries + q * qa.qstride, qb);
     __syncwarp();
-    SearchOut o = warp_beam_search<DT, MT, FPL, CPL>(P, W.S, qa.skip_self ? q : (uint64_t)-1);
+    SearchOut o = warp_beam_search<DT, MT, FPL, CPL>(P, S, qa.skip_self ? q : (uint64_t)-1);
     for (uint32_t j = lane; j < qa.k; j += 32) {
       bool v = j < o.fr_n;
-      qa.ids[q * qa.k + j] = v ? (W.S.fr_id[j] & ~DD_VBIT) : DD_NONE;
-      qa.dists[q * qa.k + j] = v ? W.S.fr_d[j] : INFINITY;
+      qa.ids[q * qa.k + j] = v ? (S.fr_id[j] & ~DD_VBIT) : DD_NONE;
+      qa.dists[q * qa.k + j] = v ? S.fr_d[j] : INFINITY;
     }
     if (lane == 0) {
       if (qa.visited) qa.visited[q] = o.vis_n;
@@ -487,7 +518,7 @@ template <int DT, int MT>
 __global__ void __launch_bounds__(32) k_beam(IndexView ix, BeamArgs ba, WarpLayout lay) {
   extern __shared__ uint4 smem_raw[];
   const uint32_t lane = lane_id();
-  WarpPtrs W = carve_query((uint8_t*)smem_raw, lay);
+  const SearchSmem S = carve_query((uint8_t*)smem_raw, lay);
   const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
   for (uint64_t q = blockIdx.x; q < ba.nq; q += gridDim.x) {
     SearchParams P;
@@ -495,17 +526,17 @@ __global__ void __launch_bounds__(32) k_beam(IndexView ix, BeamArgs ba, WarpLayo
     P.d = ix.d; P.start = ba.start; P.L = ba.L; P.k = ba.k; P.cut = ba.cut; P.limit = ba.limit;
     P.degree_limit = ba.degree_limit; P.hbits = lay.hbits; P.vcap = lay.vcap;
     P.query_mode = ba.k > 0; P.keep_visited = 1; P.err = ix.err;
-    load_vec(W.S.qv, ba.queries + q * ba.qstride, qb);
+    load_vec(S.qv, ba.queries + q * ba.qstride, qb);
     __syncwarp();
-    SearchOut o = warp_beam_search<DT, MT, 16, 4>(P, W.S, (uint64_t)ba.self_ids[q]);
-    warp_sort_pairs(W.S.vis_id, W.S.vis_d, o.vis_n);
+    SearchOut o = warp_beam_search<DT, MT, 16, 4>(P, S, (uint64_t)ba.self_ids[q]);
+    warp_sort_pairs(S.vis_id, S.vis_d, o.vis_n);
     for (uint32_t j = lane; j < o.fr_n; j += 32) {
-      ba.fr_ids[q * ba.L + j] = W.S.fr_id[j] & ~DD_VBIT;
-      ba.fr_d[q * ba.L + j] = W.S.fr_d[j];
+      ba.fr_ids[q * ba.L + j] = S.fr_id[j] & ~DD_VBIT;
+      ba.fr_d[q * ba.L + j] = S.fr_d[j];
     }
     for (uint32_t j = lane; j < o.vis_n; j += 32) {
-      ba.vis_ids[q * ba.vcap + j] = W.S.vis_id[j];
-      ba.vis_d[q * ba.vcap + j] = W.S.vis_d[j];
+      ba.vis_ids[q * ba.vcap + j] = S.vis_id[j];
+      ba.vis_d[q * ba.vcap + j] = S.vis_d[j];
     }
     if (lane == 0) {
       ba.fr_n[q] = o.fr_n;
@@ -754,12 +785,10 @@ static int occupancy(K kernel, int threads, size_t smem) {
   return b > 0 ? b : 1;
 }
 
-int search_blocks_per_sm(const IndexView& ix, const WarpLayout& lay, uint32_t L, int wpc, bool build) {
+int search_blocks_per_sm(const IndexView& ix, const WarpLayout& lay, uint32_t L, int wpc) {
   size_t sm = (size_t)lay.total * wpc;
   int b = 1;
-#define OCC4(DT, MT, F, C)                                                            \
-  b = build ? occupancy(k_search_prune<DT, MT, F, C>, wpc * 32, sm)                   \
-            : occupancy(k_query<DT, MT, F, C>, wpc * 32, sm);
+#define OCC4(DT, MT, F, C) b = occupancy(k_query<DT, MT, F, C>, wpc * 32, sm);
 #define OCC(DT, MT) DD_DISPATCH_FC(L, ix.Rp, DT, MT, OCC4)
   DD_DISPATCH_DM(ix.dtype, ix.metric, OCC);
 #undef OCC
@@ -767,16 +796,60 @@ int search_blocks_per_sm(const IndexView& ix, const WarpLayout& lay, uint32_t L,
   return b;
 }
 
-void launch_search_prune(const IndexView& ix, const RoundArgs& ra, const WarpLayout& lay,
-                         int wpc, int grid, cudaStream_t st) {
-  size_t sm = (size_t)lay.total * wpc;
+// Warps per CTA of a per-warp kernel: the CTA size (up to 16 warps) that keeps
+// the most warps resident per SM, the smaller CTA on ties.
+template <typename K>
+static LaunchPlan plan_warp_kernel(K kernel, uint32_t bytes_per_warp) {
+  LaunchPlan best{1, 0};
+  static const int cand[] = {1, 2, 4, 5, 8, 16};
+  for (int wpc : cand) {
+    const size_t sm = (size_t)bytes_per_warp * wpc;
+    if (sm > 227 * 1024) break;
+    const int b = occupancy(kernel, wpc * 32, sm);
+    if (b * wpc > best.warps_per_cta * best.blocks_per_sm) best = LaunchPlan{wpc, b};
+  }
+  if (best.blocks_per_sm == 0) best.blocks_per_sm = 1;
+  return best;
+}
+
+LaunchPlan plan_search(const IndexView& ix, const WarpLayout& lay, uint32_t L) {
+  LaunchPlan p{1, 1};
+#define CALL4(DT, MT, F, C) p = plan_warp_kernel(k_search<DT, MT, F, C>, lay.total);
+#define CALL(DT, MT) DD_DISPATCH_FC(L, ix.Rp, DT, MT, CALL4)
+  DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
+#undef CALL
+#undef CALL4
+  return p;
+}
+
+void launch_search(const IndexView& ix, const RoundArgs& ra, const WarpLayout& lay,
+                   const LaunchPlan& plan, int grid, cudaStream_t st) {
+  const size_t sm = (size_t)lay.total * plan.warps_per_cta;
 #define CALL4(DT, MT, F, C)                                                          \
-  set_smem(k_search_prune<DT, MT, F, C>, sm);                                        \
-  k_search_prune<DT, MT, F, C><<<grid, wpc * 32, sm, st>>>(ix, ra, lay);
+  set_smem(k_search<DT, MT, F, C>, sm);                                              \
+  k_search<DT, MT, F, C><<<grid, plan.warps_per_cta * 32, sm, st>>>(ix, ra, lay);
 #define CALL(DT, MT) DD_DISPATCH_FC(ra.L, ix.Rp, DT, MT, CALL4)
   DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
 #undef CALL
 #undef CALL4
+}
+
+LaunchPlan plan_prune(const IndexView& ix, const PruneLayout& lay) {
+  LaunchPlan p{1, 1};
+#define CALL(DT, MT) p = plan_warp_kernel(k_prune<DT, MT>, lay.total);
+  DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
+#undef CALL
+  return p;
+}
+
+void launch_prune_round(const IndexView& ix, const RoundArgs& ra, const PruneLayout& lay,
+                        uint32_t vcap, const LaunchPlan& plan, int grid, cudaStream_t st) {
+  const size_t sm = (size_t)lay.total * plan.warps_per_cta;
+#define CALL(DT, MT)                                                                 \
+  set_smem(k_prune<DT, MT>, sm);                                                     \
+  k_prune<DT, MT><<<grid, plan.warps_per_cta * 32, sm, st>>>(ix, ra, lay, vcap);
+  DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
+#undef CALL
 }
 
 void launch_apply_rows(const IndexView& ix, const RoundArgs& ra, cudaStream_t st) {

@@ -14,8 +14,20 @@ struct WarpLayout {
   uint32_t qv, fr_id, fr_d, c_id, c_d, s_id, s_d, vis_id, vis_d, ws;
   uint32_t total;
   uint32_t vcap;   // visited / evicted list capacity
-  uint32_t ccap;   // prune candidate capacity (the visited arrays hold vcap + Rp)
+  uint32_t ccap;   // prune candidate capacity (visited list + out-list)
   uint32_t hbits;  // hash bits of the largest beam width of the launch
+  uint32_t h24;    // hash table of 24-bit ids (every id < 0xFFFFFF)
+};
+
+// Per-warp shared-memory carve-up of k_prune (byte offsets, 16-byte aligned).
+struct PruneLayout {
+  uint32_t qv, cid, ckey, ws, total, ccap;
+};
+
+// CTA shape of a one-warp-per-item kernel
+struct LaunchPlan {
+  int warps_per_cta;
+  int blocks_per_sm;
 };
 
 struct IndexView {
@@ -30,10 +42,10 @@ struct IndexView {
 };
 
 WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, uint32_t vcap,
-                              bool with_prune);
-// warps resident per SM for a layout (occupancy of the search kernels)
-int search_blocks_per_sm(const IndexView& ix, const WarpLayout& lay, uint32_t L, int wpc,
-                         bool build);
+                              bool build, bool h24);
+PruneLayout make_prune_layout(uint32_t d, int dtype, uint32_t Rp, uint32_t ccap);
+// CTAs of k_query resident per SM for a layout
+int search_blocks_per_sm(const IndexView& ix, const WarpLayout& lay, uint32_t L, int wpc);
 
 struct RoundArgs {
   uint64_t floor;
@@ -42,9 +54,9 @@ struct RoundArgs {
   double alpha;
   uint32_t start;
   uint32_t* new_out;     // B x Rp
-  uint32_t* stat_vis;    // B (may be null)
+  uint32_t* stat_vis;    // B visited-list lengths (k_search writes, k_prune reads)
   uint32_t* stat_cmps;   // B (may be null)
-  uint32_t* vis_arena;   // per resident warp: vcap visited ids, then vcap distances
+  uint32_t* vis_all;     // per batch point: vcap visited ids, then vcap distances
 };
 
 // The round's reverse edges grouped by target (see semisort.cuh): segment k
@@ -73,8 +85,12 @@ constexpr uint32_t kRevWarps = 2;       // warps per CTA of the reverse kernel
 constexpr uint32_t kBigThreads = 512;   // threads per CTA of the big-target path
 constexpr uint32_t kBigSlots = 148;     // CTAs (and workspace slices) of the big-target path
 
-void launch_search_prune(const IndexView& ix, const RoundArgs& ra, const WarpLayout& lay,
-                         int warps_per_cta, int grid, cudaStream_t st);
+LaunchPlan plan_search(const IndexView& ix, const WarpLayout& lay, uint32_t L);
+void launch_search(const IndexView& ix, const RoundArgs& ra, const WarpLayout& lay,
+                   const LaunchPlan& plan, int grid, cudaStream_t st);
+LaunchPlan plan_prune(const IndexView& ix, const PruneLayout& lay);
+void launch_prune_round(const IndexView& ix, const RoundArgs& ra, const PruneLayout& lay,
+                        uint32_t vcap, const LaunchPlan& plan, int grid, cudaStream_t st);
 void launch_apply_rows(const IndexView& ix, const RoundArgs& ra, cudaStream_t st);
 // append-or-prune per target over the segments the semisort produced
 void launch_reverse(const IndexView& ix, const RoundArgs& ra, const ReverseScratch& rs,

@@ -46,8 +46,37 @@ struct SearchSmem {
   uint32_t* vis_id;   // visited list in visit order (keep_visited), capacity vcap
   float* vis_d;
   uint32_t* ev_id;    // visited ids pushed out of the frontier (query_mode), capacity vcap
-  uint32_t* hash;     // 2^bits slots (global memory, this warp's slice)
+  uint32_t* hash;     // 2^bits slots (shared memory): uint32 ids, or with h24
+                      // a uint16 array of the low bits then a uint8 array of the high bits
+  int h24;            // ids stored in 24 bits (every id < 0xFFFFFF); 0xFFFFFF = empty
 };
+
+// bytes of the lossy "seen" table of 2^hbits slots
+__host__ __device__ inline uint32_t hash_table_bytes(uint32_t hbits, bool h24) {
+  return (h24 ? 3u : 4u) << hbits;
+}
+
+// the id a slot holds (DD_NONE when empty); h24 is warp-uniform
+__device__ __forceinline__ uint32_t hash_get(const SearchSmem& S, uint32_t nslots, uint32_t slot) {
+  if (S.h24) {
+    const uint16_t* lo = (const uint16_t*)S.hash;
+    const uint8_t* hi = (const uint8_t*)(lo + nslots);
+    const uint32_t v = (uint32_t)lo[slot] | ((uint32_t)hi[slot] << 16);
+    return v == 0xFFFFFFu ? DD_NONE : v;
+  }
+  return S.hash[slot];
+}
+__device__ __forceinline__ void hash_set(const SearchSmem& S, uint32_t nslots, uint32_t slot,
+                                         uint32_t id) {
+  if (S.h24) {
+    uint16_t* lo = (uint16_t*)S.hash;
+    uint8_t* hi = (uint8_t*)(lo + nslots);
+    lo[slot] = (uint16_t)(id & 0xFFFFu);
+    hi[slot] = (uint8_t)(id >> 16);
+  } else {
+    S.hash[slot] = id;
+  }
+}
 
 struct SearchParams {
   const uint8_t* points;
@@ -111,9 +140,11 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
   const uint32_t nslots = 1u << P.hbits;
   const uint32_t hmask = nslots - 1;
   {
+    // all-ones bytes are the empty marker of both layouts
     uint4* h4 = (uint4*)S.hash;
     const uint4 none = make_uint4(DD_NONE, DD_NONE, DD_NONE, DD_NONE);
-    for (uint32_t i = lane; i < nslots / 4; i += 32) h4[i] = none;
+    const uint32_t n16 = hash_table_bytes(P.hbits, S.h24 != 0) / 16u;
+    for (uint32_t i = lane; i < n16; i += 32) h4[i] = none;
   }
   if (lane == 0) {
     S.fr_id[0] = P.start;
@@ -205,12 +236,12 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
       uint32_t loc = part ? (uint32_t)(dd_hash64(at) & hmask) : (0x80000000u | lane);
       uint32_t grp = __match_any_sync(FULL, loc);
       uint32_t before = grp & lanemask_lt();
-      uint32_t tval = part ? S.hash[loc] : DD_NONE;
+      uint32_t tval = part ? hash_get(S, nslots, loc) : DD_NONE;
       uint32_t prev_a = __shfl_sync(FULL, at, before ? 31 - __clz(before) : lane);
       uint32_t seen_val = before ? prev_a : tval;
       keep[t] = part && (seen_val != at);
       __syncwarp();
-      if (part && (grp & lanemask_gt()) == 0) S.hash[loc] = at;
+      if (part && (grp & lanemask_gt()) == 0) hash_set(S, nslots, loc, at);
       __syncwarp();
     }
 

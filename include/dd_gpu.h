@@ -73,6 +73,8 @@ typedef struct dd_stats {
   double build_ms;         /* device time of the whole build */
   double search_prune_ms;  /* device time of the insert search + prune kernels */
   double reverse_ms;       /* device time of the reverse-edge kernels */
+  double search_ms;        /* device time of the insert beam searches alone (part of
+                              search_prune_ms) */
 } dd_stats;
 
 /* ------------------------------------------------------------------ handle */
