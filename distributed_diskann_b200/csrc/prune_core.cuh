@@ -140,11 +140,70 @@ __device__ __forceinline__ void warp_partition_loop(const ddsort::Arr<uint32_t>&
   }
 }
 
+// Fast path of warp_std_sort for lists without equal keys, where std::sort's
+// result is the one ascending order.  Returns false (list untouched) when two
+// keys are equal.  A list already in strictly ascending order is left as is
+// (a sorted list with equal neighbours goes straight back to the caller);
+// otherwise each element's rank (count of smaller keys) is its position, and
+// the list is rewritten through the rank-pairing scratch (2 * cap ints).
+constexpr uint32_t kRankSortMax = 256;
+__device__ __forceinline__ bool warp_sort_distinct(const PruneSmem& S, uint32_t m) {
+  const uint32_t FULL = 0xffffffffu;
+  const uint32_t lane = lane_id();
+  bool strict = true, nondesc = true;
+  for (uint32_t b = 1; b < m && nondesc; b += 32) {
+    const uint32_t i = b + lane;
+    const float k0 = i < m ? S.ckey[i - 1] : 0.f, k1 = i < m ? S.ckey[i] : 1.f;
+    strict = __all_sync(FULL, !strict ? false : k0 < k1) && strict;
+    nondesc = __all_sync(FULL, k0 <= k1);
+  }
+  if (strict && nondesc) return true;
+  if (nondesc || m > kRankSortMax) return false;
+  uint32_t rk[kRankSortMax / 32];
+  bool tie = false;
+#pragma unroll
+  for (int t = 0; t < (int)(kRankSortMax / 32); t++) {
+    const uint32_t i = lane + 32u * t;
+    rk[t] = 0;
+    if (i < m) {
+      const float ki = S.ckey[i];
+      uint32_t r = 0, eq = 0;
+      for (uint32_t j = 0; j < m; j++) {
+        const float kj = S.ckey[j];
+        r += kj < ki ? 1u : 0u;
+        eq += kj == ki ? 1u : 0u;
+      }
+      rk[t] = r;
+      tie |= eq != 1u;
+    }
+  }
+  if (__any_sync(FULL, tie)) return false;
+  int* tid = S.posL;
+  float* tkey = (float*)S.posR;
+#pragma unroll
+  for (int t = 0; t < (int)(kRankSortMax / 32); t++) {
+    const uint32_t i = lane + 32u * t;
+    if (i < m) {
+      tid[rk[t]] = (int)S.cid[i];
+      tkey[rk[t]] = S.ckey[i];
+    }
+  }
+  __syncwarp();
+  for (uint32_t i = lane; i < m; i += 32) {
+    S.cid[i] = (uint32_t)tid[i];
+    S.ckey[i] = tkey[i];
+  }
+  __syncwarp();
+  return true;
+}
+
 // Orders cid/ckey[0, m) exactly like std::sort with the distance-only
-// comparator: the warp replays the partition phase, marking leaf starts in a
-// bitmap; then the lanes finish the leaves in parallel.
+// comparator: lists without equal keys take warp_sort_distinct; otherwise
+// the warp replays the partition phase, marking leaf starts in a bitmap, and
+// the lanes finish the leaves in parallel.
 __device__ __forceinline__ void warp_std_sort(const PruneSmem& S, uint32_t m) {
   const uint32_t lane = lane_id();
+  if (warp_sort_distinct(S, m)) return;
   ddsort::Arr<uint32_t> A{S.cid, S.ckey};
   const uint32_t nw = (m + 31) / 32;
   for (uint32_t w = lane; w < nw; w += 32) S.leafbits[w] = 0;

@@ -152,6 +152,7 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
   }
   __syncwarp();
   uint32_t fr_n = 1;
+  uint32_t scan0 = 0;      // lower bound of the first unvisited frontier position
   uint32_t vis_n = 0;      // visited list length
   uint32_t ev_n = 0;       // evicted list length (query mode)
   uint32_t cmps = 1;       // dist to the start point
@@ -174,9 +175,9 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
   };
 
   while (num_visited < P.limit) {
-    // ---- closest unvisited frontier entry
+    // ---- closest unvisited frontier entry (every entry before scan0 is visited)
     int cur_pos = -1;
-    for (uint32_t base = 0; base < fr_n; base += 32) {
+    for (uint32_t base = scan0 & ~31u; base < fr_n; base += 32) {
       uint32_t i = base + lane;
       bool unv = (i < fr_n) && !(S.fr_id[i] & DD_VBIT);
       uint32_t b = __ballot_sync(FULL, unv);
@@ -222,27 +223,41 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
       if (b) { nxt_pos = (int)(base + __ffs(b) - 1); break; }
     }
 
-    // ---- hash filter, replayed chunk by chunk in neighbour order
+    // ---- hash filter, replayed chunk by chunk in neighbour order.  The
+    // slots, same-slot groups and predecessor ids of all chunks are computed
+    // first (they do not depend on the table); the table is then read and
+    // written chunk after chunk.
     bool keep[CPL];
+    {
+      bool part[CPL];
+      uint32_t loc[CPL], grp[CPL], prev_a[CPL];
 #pragma unroll
-    for (int t = 0; t < CPL; t++) {
-      uint32_t at = a[t];
-      if (at != DD_NONE && at >= P.n) {
-        dd_set_error(P.err, DD_EBAD_ID);
-        at = DD_NONE;
-        a[t] = DD_NONE;
+      for (int t = 0; t < CPL; t++) {
+        uint32_t at = a[t];
+        if (at != DD_NONE && at >= P.n) {
+          dd_set_error(P.err, DD_EBAD_ID);
+          at = DD_NONE;
+          a[t] = DD_NONE;
+        }
+        part[t] = (at != DD_NONE) && ((uint64_t)at != self_id);
+        loc[t] = part[t] ? (uint32_t)(dd_hash64(at) & hmask) : (0x80000000u | lane);
       }
-      bool part = (at != DD_NONE) && ((uint64_t)at != self_id);
-      uint32_t loc = part ? (uint32_t)(dd_hash64(at) & hmask) : (0x80000000u | lane);
-      uint32_t grp = __match_any_sync(FULL, loc);
-      uint32_t before = grp & lanemask_lt();
-      uint32_t tval = part ? hash_get(S, nslots, loc) : DD_NONE;
-      uint32_t prev_a = __shfl_sync(FULL, at, before ? 31 - __clz(before) : lane);
-      uint32_t seen_val = before ? prev_a : tval;
-      keep[t] = part && (seen_val != at);
-      __syncwarp();
-      if (part && (grp & lanemask_gt()) == 0) hash_set(S, nslots, loc, at);
-      __syncwarp();
+#pragma unroll
+      for (int t = 0; t < CPL; t++) {
+        grp[t] = __match_any_sync(FULL, loc[t]);
+        const uint32_t before = grp[t] & lanemask_lt();
+        prev_a[t] = __shfl_sync(FULL, a[t], before ? 31 - __clz(before) : lane);
+      }
+#pragma unroll
+      for (int t = 0; t < CPL; t++) {
+        const uint32_t before = grp[t] & lanemask_lt();
+        const uint32_t tval = (part[t] && !before) ? hash_get(S, nslots, loc[t]) : DD_NONE;
+        const uint32_t seen_val = before ? prev_a[t] : tval;
+        keep[t] = part[t] && (seen_val != a[t]);
+        __syncwarp();
+        if (part[t] && (grp[t] & lanemask_gt()) == 0) hash_set(S, nslots, loc[t], a[t]);
+        __syncwarp();
+      }
     }
 
     // ---- the kept neighbours, compacted in neighbour order
@@ -280,6 +295,7 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
     __syncwarp();
     if (nc == 0) {
       if (nxt_pos >= 0) prefetch_row(S.fr_id[nxt_pos]);
+      scan0 = nxt_pos >= 0 ? (uint32_t)nxt_pos : fr_n;
       continue;
     }
 
@@ -367,11 +383,18 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
         nid = S.fr_id[nxt_pos];
       if (nid != DD_NONE) prefetch_row(nid);
     }
-    if (nkeep == 0) continue;
+    if (nkeep == 0) {
+      scan0 = nxt_pos >= 0 ? (uint32_t)nxt_pos : fr_n;
+      continue;
+    }
 
     // ---- merge: frontier entry i moves to i + #(kept candidates placed before
-    // it) = i + #{j : ub_j <= i}; candidate j moves to j + ub_j
+    // it) = i + #{j : ub_j <= i}; candidate j moves to j + ub_j.  Entries
+    // before the first insertion point ub_0 stay where they are.
     const uint32_t new_n = min(P.L, fr_n + nkeep);
+    const uint32_t ub0 = S.s_id[0];
+    // unvisited entries now sit at or after min(ub_0, old nxt_pos)
+    scan0 = min(ub0, nxt_pos >= 0 ? (uint32_t)nxt_pos : new_n);
     uint32_t my_id[FPL], my_pos[FPL];
     float my_d[FPL];
 #pragma unroll
@@ -381,15 +404,19 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
       my_id[t] = 0;
       my_d[t] = 0.f;
       if (i < fr_n) {
-        uint32_t lo = 0, hi = nkeep;
-        while (lo < hi) {
-          uint32_t mid = (lo + hi) >> 1;
-          if (S.s_id[mid] <= i) lo = mid + 1;
-          else hi = mid;
+        if (i < ub0) {
+          my_pos[t] = i;  // unmoved: not rewritten
+        } else {
+          uint32_t lo = 1, hi = nkeep;
+          while (lo < hi) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (S.s_id[mid] <= i) lo = mid + 1;
+            else hi = mid;
+          }
+          my_id[t] = S.fr_id[i];
+          my_d[t] = S.fr_d[i];
+          my_pos[t] = i + lo;
         }
-        my_id[t] = S.fr_id[i];
-        my_d[t] = S.fr_d[i];
-        my_pos[t] = i + lo;
       }
     }
     uint32_t c_ids[CPL], c_pos[CPL];
@@ -409,7 +436,7 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
     __syncwarp();
 #pragma unroll
     for (int t = 0; t < FPL; t++) {
-      if (my_pos[t] < new_n) {
+      if (my_pos[t] < new_n && my_pos[t] != lane + 32u * t) {
         S.fr_id[my_pos[t]] = my_id[t];
         S.fr_d[my_pos[t]] = my_d[t];
       }
