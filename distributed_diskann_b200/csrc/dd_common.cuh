@@ -50,6 +50,7 @@ struct Dist<DD_F32, DD_L2> {
     const float4* b4 = (const float4*)bv;
     float r = 0.f;
     uint32_t i = 0;
+#pragma unroll 8
     for (; i + 3 < d; i += 4) {
       float4 x = *(const float4*)(a + i);
       float4 y = __ldg(b4 + (i >> 2));
@@ -76,6 +77,7 @@ struct Dist<DD_F32, DD_MIPS> {
     const float4* b4 = (const float4*)bv;
     float r = 0.f;
     uint32_t i = 0;
+#pragma unroll 8
     for (; i + 3 < d; i += 4) {
       float4 x = *(const float4*)(a + i);
       float4 y = __ldg(b4 + (i >> 2));
@@ -104,6 +106,7 @@ struct DistIntL2 {
     const uint4* b = (const uint4*)bv;
     uint32_t acc = 0;
     uint32_t nv = (d + 15) >> 4;
+#pragma unroll 8
     for (uint32_t i = 0; i < nv; i++) {
       uint4 x = a[i];
       uint4 y = __ldg(b + i);
@@ -124,6 +127,7 @@ struct DistIntIP {
     const uint4* b = (const uint4*)bv;
     int acc = 0;
     uint32_t nv = (d + 15) >> 4;
+#pragma unroll 8
     for (uint32_t i = 0; i < nv; i++) {
       uint4 x = a[i];
       uint4 y = __ldg(b + i);

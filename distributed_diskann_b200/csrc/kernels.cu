@@ -318,12 +318,21 @@ __global__ void __launch_bounds__(kRevWarps * 32, 7) k_reverse(IndexView ix, Rou
 
 // Targets with more than kRevCandCap candidates: one CTA each, candidates in
 // this CTA's global workspace slice.  The sort emulation splits the work:
-// ranges longer than kCtaRange are partitioned by the whole CTA, shorter ones
+// ranges longer than cta_range are partitioned by the whole CTA, shorter ones
 // by single warps; then all threads finish the leaves.  The greedy selection
 // spreads each occlusion pass over the CTA and compacts the survivors while
 // the list is long.
-constexpr int kCtaRange = 4096;
+//
+// The short ranges are recorded in `ranges` (room for cap/8 + 64 records).
+// Ranges longer than K at one recursion depth are disjoint and the depth is
+// at most 2 log2(m), so there are at most (m / K) * 2 log2(m) + 1 records:
+// K = 256 keeps that within m/8 + 1 for m <= 65536, K = 1024 for every m
+// below 2^32.
+__device__ __forceinline__ int big_cta_range(uint32_t m) { return m <= 65536u ? 256 : 1024; }
 constexpr int kBigStackInts = 3 * 72;
+// mma_sel_bytes(kMaxRp): staged rows, norms and thresholds of the warp greedy
+constexpr uint32_t kBigSelBytes = (kMaxRp + kMmaChunk) * 128u + (kMaxRp + kMmaChunk) * 4u +
+                                  kMmaChunk * 4u;
 
 template <int DT, int MT>
 __global__ void __launch_bounds__(kBigThreads) k_reverse_big(IndexView ix, RoundArgs ra, ReverseScratch rs) {
@@ -332,6 +341,8 @@ __global__ void __launch_bounds__(kBigThreads) k_reverse_big(IndexView ix, Round
   __shared__ int cstack[kBigStackInts];
   __shared__ int wstack[kBigThreads / 32][kBigStackInts];
   __shared__ uint32_t s_deg, s_nsmall, s_next, s_mm;
+  // rows and norms of the tensor-core greedy (integer data, rows <= 128 bytes)
+  __shared__ __align__(16) uint8_t gsel[kBigSelBytes];
   const uint32_t tid = threadIdx.x, lane = lane_id(), wid = tid >> 5;
   const uint64_t cap = rs.gcap;
   const uint64_t slot = blockIdx.x;
@@ -385,12 +396,13 @@ __global__ void __launch_bounds__(kBigThreads) k_reverse_big(IndexView ix, Round
     }
     __syncthreads();
     // ---- sort emulation, phase 1: long ranges, whole CTA
+    const int cta_range = big_cta_range(m);
     int sp = 3;
     while (sp > 0) {
       int depth = cstack[sp - 1], last = cstack[sp - 2], first = cstack[sp - 3];
       sp -= 3;
       __syncthreads();
-      while (last - first > kCtaRange && depth > 0) {
+      while (last - first > cta_range && depth > 0) {
         --depth;
         const int mid = first + (last - first) / 2;
         if (tid == 0) ddsort::move_median_to_first(A, first, first + 1, mid, last - 1);
@@ -430,6 +442,24 @@ __global__ void __launch_bounds__(kBigThreads) k_reverse_big(IndexView ix, Round
         ddsort::insertion_sort_range(A, (int)q, ddsort::leaf_end(bits, (int)q, (int)m));
     __syncthreads();
     // ---- greedy selection (the row of t is rewritten; its old entries are in cid)
+    if (DT != DD_F32 && greedy_uses_mma(ix.d, DT)) {
+      // chunked greedy on one warp: every candidate row is read once, and the
+      // walk stops at the R-th selection (hub lists are far longer than that)
+      if (wid == 0) {
+        PruneSmem Pg{};
+        Pg.cid = cid;
+        Pg.ckey = ckey;
+        Pg.sel = (uint4*)gsel;
+        warp_greedy_select_mma<DT, MT>(ix.points, ix.stride, ix.d, t, Pg, m, ra.alpha, ix.R, row,
+                                       ix.Rp, Pg.sel);
+        if (lane == 0) {
+          atomicAdd(&rs.counters[2], 1u);
+          atomicAdd(&rs.counters[3], m);
+        }
+      }
+      __syncthreads();
+      continue;
+    }
     uint32_t nsel = 0, idx = 0, mm = m;
     while (nsel < ix.R && idx < mm) {
       const uint32_t ps = cid[idx];

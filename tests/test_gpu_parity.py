@@ -164,11 +164,25 @@ def test_two_pass_graphs_and_their_queries_vs_oracle(oracle_mod, R, L, metric):
 
 
 def test_mid_size_int8_build_bit_exact_vs_oracle(oracle_mod):
-    """100k x 100 int8 (the reference's own measured case) against the oracle."""
+    """100k x 100 int8 (the reference's own measured case) against the oracle.
+    The start point collects more than 512 reverse-edge candidates, so the
+    hub-target path (one CTA per target) is part of the comparison."""
     base = D.gen_mixture_i8(100_000, 100, 1000, 4)
     gi, graph, st = gpu_build(base, 64, 128, 1.2)
     og, ost = oracle_mod.build(base, 64, 128, 1.2)
     np.testing.assert_array_equal(graph, canon(og))
+    assert st["big_groups"] > 0 and st["reverse_prunes"] > 0
+    gi.close()
+
+
+def test_mid_size_uint8_build_bit_exact_vs_oracle(oracle_mod):
+    """120k x 128 uint8 with the skewed non-negative values of the BIGANN-shaped
+    workload (u8 x u8 tensor-core tiles), hub targets included."""
+    base = D.gen_skewed_u8(120_000, 128, 1200, 6)
+    gi, graph, st = gpu_build(base, 64, 128, 1.2)
+    og, ost = oracle_mod.build(base, 64, 128, 1.2)
+    np.testing.assert_array_equal(graph, canon(og))
+    assert st["big_groups"] > 0 and st["reverse_prunes"] > 0
     gi.close()
 
 
