@@ -54,6 +54,7 @@ struct dd_index {
   // per-point visited-list slices of the build searches (grown on demand)
   uint32_t* vis_all = nullptr;
   uint64_t vis_all_words = 0;
+  uint32_t* ref_rows = nullptr;  // n x (R+1) reference-layout rows for downloads
   bool verbose = false;
 };
 
@@ -395,7 +396,7 @@ int dd_destroy(dd_index* h) {
   void* ptrs[] = {h->points, h->graph, h->err, h->new_out, h->stat_vis, h->stat_cmps,
                   h->sort_t[0], h->sort_t[1], h->sort_v[0], h->sort_v[1], h->hist, h->heads,
                   h->flags, h->counters, h->big, h->block_sums, h->acc, h->gcand, h->gkey,
-                  h->gpos, h->gbits, h->granges, h->vis_all};
+                  h->gpos, h->gbits, h->granges, h->vis_all, h->ref_rows};
   for (void* p : ptrs) dfree(p);
   delete h;
   return DD_OK;
@@ -466,14 +467,12 @@ int dd_upload_graph(dd_index* h, const uint32_t* rows) {
 int dd_download_graph(dd_index* h, uint32_t* rows) {
   if (!h || !rows) return DD_ERR_ARG;
   CK(cudaSetDevice(h->device));
-  uint32_t* tmp = nullptr;
-  CK(dalloc(&tmp, h->n * (h->R + 1)));
-  launch_to_ref_rows(view(h), tmp, h->stream);
-  cudaError_t e = cudaMemcpyAsync(rows, tmp, h->n * (h->R + 1) * 4ull, cudaMemcpyDeviceToHost,
-                                  h->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-  cudaFree(tmp);
-  CK(e);
+  // the reference-layout rows are assembled in a buffer kept by the handle
+  if (!h->ref_rows) CK(dalloc(&h->ref_rows, h->n * (h->R + 1)));
+  launch_to_ref_rows(view(h), h->ref_rows, h->stream);
+  CK(cudaMemcpyAsync(rows, h->ref_rows, h->n * (h->R + 1) * 4ull, cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
   return DD_OK;
 }
 
