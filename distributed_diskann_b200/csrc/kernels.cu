@@ -281,8 +281,9 @@ __device__ void reverse_one(const IndexView& ix, const RoundArgs& ra, const Reve
   __syncwarp();
   const uint32_t m = s + deg;
   warp_std_sort(Pm, m);
-  warp_greedy_select_fast<DT, MT>(ix.points, ix.stride, ix.d, t, Pm, m, ra.alpha, ix.R, row, ix.Rp,
-                                  Pm.sel);
+  // the candidate rows were just read for their distances to t: no prefetch
+  warp_greedy_select_fast<DT, MT, false>(ix.points, ix.stride, ix.d, t, Pm, m, ra.alpha, ix.R, row,
+                                         ix.Rp, Pm.sel);
   if (lane == 0) {
     atomicAdd(&rs.counters[2], 1u);
     atomicAdd(&rs.counters[3], m);

@@ -197,10 +197,47 @@ __device__ __forceinline__ bool warp_sort_distinct(const PruneSmem& S, uint32_t 
   return true;
 }
 
+// Leaf phase of the emulation: the library's final insertion sort is a
+// stable sort inside each leaf.  Leaves of more than kThreshold elements are
+// heap-sorted ranges (already ascending); in the others each element's place
+// is its stable rank within the leaf, computed by all lanes in parallel.  The
+// permuted list goes through the rank-pairing scratch (2 * cap ints).
+__device__ __forceinline__ void warp_finish_leaves(const PruneSmem& S, uint32_t m) {
+  const uint32_t lane = lane_id();
+  int* tid = S.posL;
+  float* tkey = (float*)S.posR;
+  for (uint32_t i = lane; i < m; i += 32) {
+    // leaf start: the last marked position <= i
+    int w = (int)(i >> 5);
+    uint32_t bw = S.leafbits[w] & (0xffffffffu >> (31 - (i & 31)));
+    while (bw == 0 && w > 0) bw = S.leafbits[--w];
+    const int lo = (w << 5) + 31 - __clz(bw);
+    const int hi = ddsort::leaf_end(S.leafbits, lo, (int)m);
+    const float ki = S.ckey[i];
+    uint32_t dst = i;
+    if (hi - lo <= ddsort::kThreshold) {
+      uint32_t r = 0;
+      for (int j = lo; j < hi; j++) {
+        const float kj = S.ckey[j];
+        r += (kj < ki || (kj == ki && j < (int)i)) ? 1u : 0u;
+      }
+      dst = (uint32_t)lo + r;
+    }
+    tid[dst] = (int)S.cid[i];
+    tkey[dst] = ki;
+  }
+  __syncwarp();
+  for (uint32_t i = lane; i < m; i += 32) {
+    S.cid[i] = (uint32_t)tid[i];
+    S.ckey[i] = tkey[i];
+  }
+  __syncwarp();
+}
+
 // Orders cid/ckey[0, m) exactly like std::sort with the distance-only
 // comparator: lists without equal keys take warp_sort_distinct; otherwise
 // the warp replays the partition phase, marking leaf starts in a bitmap, and
-// the lanes finish the leaves in parallel.
+// the leaves are finished in parallel (warp_finish_leaves).
 __device__ __forceinline__ void warp_std_sort(const PruneSmem& S, uint32_t m) {
   const uint32_t lane = lane_id();
   if (warp_sort_distinct(S, m)) return;
@@ -211,10 +248,7 @@ __device__ __forceinline__ void warp_std_sort(const PruneSmem& S, uint32_t m) {
   if (m > 0)
     warp_partition_loop(A, 0, (int)m, 2 * ddsort::floor_log2((int)m), S.stack, S.leafbits, S.posL,
                         S.posR, false);
-  for (uint32_t i = lane; i < m; i += 32)
-    if (S.leafbits[i >> 5] & (1u << (i & 31)))
-      ddsort::insertion_sort_range(A, (int)i, ddsort::leaf_end(S.leafbits, (int)i, (int)m));
-  __syncwarp();
+  warp_finish_leaves(S, m);
 }
 
 // CTA-wide sum (all threads call it; sh: 32 words)
@@ -570,7 +604,9 @@ __device__ __forceinline__ uint32_t gather_nibble_bits(uint32_t x) {
   return x;
 }
 
-template <int DT, int MT>
+// PREFETCH: load the next chunk's rows while the current chunk's tiles run
+// (worth it when the rows are not in cache yet).
+template <int DT, int MT, bool PREFETCH = true>
 __device__ uint32_t warp_greedy_select_mma(const uint8_t* points, uint64_t stride, uint32_t d,
                                            uint32_t p, const PruneSmem& S, uint32_t m,
                                            double alpha, uint32_t R, uint32_t* out_row,
@@ -583,21 +619,38 @@ __device__ uint32_t warp_greedy_select_mma(const uint8_t* points, uint64_t strid
   const uint32_t qb = (d + 15u) & ~15u;   // padded row bytes (integer data)
   const uint32_t KS = (qb + 31u) >> 5;    // k-steps of 32 bytes
   const uint32_t NW = 2u * KS;            // 16-byte words staged per row
+  // A chunk's rows are loaded into registers (two lanes per member, 16-byte
+  // words h, h+2, h+4, h+6): with PREFETCH one chunk ahead of its tiles.
+  uint4 pv[4];
+  uint32_t pcj = DD_NONE;
+  auto load_chunk = [&](uint32_t c0) {
+    const uint32_t j = lane >> 1, h = lane & 1;
+    const uint32_t cnt = c0 < m ? min(kMmaChunk, m - c0) : 0u;
+    pcj = j < cnt ? S.cid[c0 + j] : DD_NONE;
+    const bool alive = pcj != DD_NONE && pcj != p;
+    const uint4* src = (const uint4*)(points + (uint64_t)(alive ? pcj : 0u) * stride);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const uint32_t w = h + 2u * i;
+      pv[i] = (alive && w < NW) ? __ldg(src + w) : make_uint4(0, 0, 0, 0);
+    }
+  };
+  if (PREFETCH) load_chunk(0);
   uint32_t nsel = 0;
   for (uint32_t c0 = 0; c0 < m && nsel < R; c0 += kMmaChunk) {
-    const uint32_t cnt = min(kMmaChunk, m - c0);
+    if (!PREFETCH) load_chunk(c0);
     // ---- 1. stage the chunk: two lanes per member, rows nsel .. nsel + 15
     uint32_t amask;
     {
       const uint32_t j = lane >> 1, h = lane & 1;
-      const uint32_t cj = j < cnt ? S.cid[c0 + j] : DD_NONE;
+      const uint32_t cj = pcj;
       const bool alive = cj != DD_NONE && cj != p;
       const uint32_t r = nsel + j;
-      const uint4* src = (const uint4*)(points + (uint64_t)(alive ? cj : 0u) * stride);
       uint32_t nrm = 0;
-      for (uint32_t w = h; w < 8; w += 2) {
-        uint4 v = make_uint4(0, 0, 0, 0);
-        if (alive && w < NW) v = __ldg(src + w);
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const uint32_t w = h + 2u * i;
+        const uint4 v = pv[i];
         *mma_row_vec(rw, r, w) = v;
         if (DT == DD_U8) {
           nrm = __dp4a(v.x, v.x, nrm); nrm = __dp4a(v.y, v.y, nrm);
@@ -620,6 +673,7 @@ __device__ uint32_t warp_greedy_select_mma(const uint8_t* points, uint64_t strid
       amask = __ballot_sync(FULL, lane < kMmaChunk && a2);
     }
     __syncwarp();
+    if (PREFETCH) load_chunk(c0 + kMmaChunk);
     // ---- 2. occlusion by the entries selected before this chunk
     for (uint32_t r0 = 0; r0 < nsel && amask; r0 += 16) {
       int acc[2][4];
@@ -696,8 +750,9 @@ __device__ uint32_t warp_greedy_select_mma(const uint8_t* points, uint64_t strid
 }
 
 // The fastest exact greedy form for the data type; `sel` holds
-// greedy_sel_bytes(d, DT, Rp) bytes (unused by the generic form).
-template <int DT, int MT>
+// greedy_sel_bytes(d, DT, Rp) bytes (unused by the generic form).  PREFETCH:
+// see warp_greedy_select_mma.
+template <int DT, int MT, bool PREFETCH = true>
 __device__ __forceinline__ uint32_t warp_greedy_select_fast(const uint8_t* points, uint64_t stride,
                                                             uint32_t d, uint32_t p,
                                                             const PruneSmem& S, uint32_t m,
@@ -706,8 +761,8 @@ __device__ __forceinline__ uint32_t warp_greedy_select_fast(const uint8_t* point
                                                             uint4* sel) {
   if (DT != DD_F32) {
     if (greedy_uses_mma(d, DT))
-      return warp_greedy_select_mma<DT, MT>(points, stride, d, p, S, m, alpha, R, out_row, Rp,
-                                            sel);
+      return warp_greedy_select_mma<DT, MT, PREFETCH>(points, stride, d, p, S, m, alpha, R,
+                                                      out_row, Rp, sel);
   } else if (row_words16(d, DT) <= (uint32_t)RegRow<DT>::NVM) {
     return warp_greedy_select_reg<DT, MT>(points, stride, d, p, S, m, alpha, R, out_row, Rp, sel);
   }
