@@ -291,7 +291,7 @@ __device__ void reverse_one(const IndexView& ix, const RoundArgs& ra, const Reve
 }
 
 template <int DT, int MT>
-__global__ void __launch_bounds__(kRevWarps * 32, 7) k_reverse(IndexView ix, RoundArgs ra, ReverseScratch rs) {
+__global__ void __launch_bounds__(kRevWarps * 32, 8) k_reverse(IndexView ix, RoundArgs ra, ReverseScratch rs) {
   extern __shared__ uint4 smem_raw[];
   const RevLayout L = rev_layout(ix.d, DT, ix.Rp);
   const uint32_t wic = threadIdx.x >> 5, lane = lane_id();

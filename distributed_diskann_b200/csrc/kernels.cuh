@@ -80,7 +80,7 @@ struct ReverseScratch {
 constexpr int kScanBlocks = 512;
 // stack room of the sort emulation for any list length below 2^32
 constexpr int kGlobalStackInts = 3 * (2 * 32 + 4);
-constexpr uint32_t kRevCandCap = 512;   // per-warp shared-memory candidates (reverse)
+constexpr uint32_t kRevCandCap = 256;   // per-warp shared-memory candidates (reverse)
 constexpr uint32_t kRevWarps = 2;       // warps per CTA of the reverse kernel
 constexpr uint32_t kBigThreads = 512;   // threads per CTA of the big-target path
 constexpr uint32_t kBigSlots = 148;     // CTAs (and workspace slices) of the big-target path

@@ -165,7 +165,7 @@ def test_two_pass_graphs_and_their_queries_vs_oracle(oracle_mod, R, L, metric):
 
 def test_mid_size_int8_build_bit_exact_vs_oracle(oracle_mod):
     """100k x 100 int8 (the reference's own measured case) against the oracle.
-    The start point collects more than 512 reverse-edge candidates, so the
+    The start point collects more than 256 reverse-edge candidates, so the
     hub-target path (one CTA per target) is part of the comparison."""
     base = D.gen_mixture_i8(100_000, 100, 1000, 4)
     gi, graph, st = gpu_build(base, 64, 128, 1.2)
