@@ -190,6 +190,7 @@ def main():
     import torch.distributed as dist
 
     from distributed_diskann_b200 import datasets as D
+    from distributed_diskann_b200 import multirank as MR
     from distributed_diskann_b200.index import GpuIndex
 
     torch.cuda.set_device(local_rank)
@@ -202,9 +203,7 @@ def main():
     n = args.n or w.n
     nq = args.nq or w.nq
     # each rank builds its own partition (different seed) of the same size
-    import dataclasses
-
-    wr = dataclasses.replace(w, seed=w.seed + 1000 * rank)
+    wr = MR.rank_workload(w, rank)
     t0 = time.time()
     base, queries = D.make_workload(wr, n=n, nq=nq)
     gen_s = time.time() - t0
@@ -222,10 +221,7 @@ def main():
         torch.cuda.synchronize(dev)
 
     def max_over_ranks(x):
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return MR.max_over_ranks(x, dev, world > 1)
 
     # ---- warm-up
     for _ in range(args.warmup):
@@ -233,8 +229,7 @@ def main():
     barrier()
 
     # ---- timed builds, inputs resident in HBM
-    gpu_index = os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)).split(",")[local_rank]
-    clocks = ClockSampler(gpu_index)
+    clocks = ClockSampler(MR.gpu_index(local_rank))
     clocks.start()
     launches = 0
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -248,7 +243,7 @@ def main():
     t_dev = ev0.elapsed_time(ev1) / 1000.0
     clk = clocks.stop()
     t_max = max_over_ranks(t_dev)
-    value = world * n * args.steps / t_max
+    value = MR.whole_job_rate(world, n, args.steps, t_max)
 
     # ---- e2e through the C ABI with host buffers
     barrier()
@@ -260,7 +255,7 @@ def main():
     ev1.record(stream)
     ev1.synchronize()
     t_e2e = max_over_ranks(ev0.elapsed_time(ev1) / 1000.0)
-    e2e_value = world * n * args.steps / t_e2e
+    e2e_value = MR.whole_job_rate(world, n, args.steps, t_e2e)
     h2d = base.nbytes
     d2h = n * (w.R + 1) * 4
 
@@ -307,7 +302,7 @@ def main():
         for L in w.sweep_L:
             Ls = torch.full((nq,), L, dtype=torch.int32, device=dev)
             for _ in range(2):  # first run warms up; the second is timed (checkRecall)
-                barrier()
+                torch.cuda.synchronize(dev)  # rank 0 only: no collective here
                 ev0.record(stream)
                 gi.search_device(qpad.data_ptr(), nq, qstride, Ls.data_ptr(), L, k,
                                  ids.data_ptr(), dd.data_ptr())
@@ -318,7 +313,7 @@ def main():
             sweep.append({"L": L, "qps": nq / t, "recall10": rec})
         Ls = torch.tensor(np.array(w.sweep_L, np.int32)[np.arange(nq) % len(w.sweep_L)],
                           device=dev)
-        barrier()
+        torch.cuda.synchronize(dev)
         ev0.record(stream)
         gi.search_device(qpad.data_ptr(), nq, qstride, Ls.data_ptr(), max(w.sweep_L), k,
                          ids.data_ptr(), dd.data_ptr())
