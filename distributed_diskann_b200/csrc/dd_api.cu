@@ -616,13 +616,14 @@ int dd_search_device(dd_index* h, const void* queries, uint64_t nq, uint64_t qst
   if (qstride % 16) return fail(h, DD_ERR_ARG, "device query stride must be a multiple of 16");
   CK(cudaSetDevice(h->device));
   h->launches = 0;
-  WarpLayout lay = make_search_layout(h->d, h->dtype, Lmax, h->Rp, 2 * Lmax + 64, false, use_h24(h));
-  int wpc = 4;
-  while (wpc > 1 && (size_t)lay.total * wpc > 227 * 1024) wpc >>= 1;
-  if ((size_t)lay.total * wpc > 227 * 1024)
+  WarpLayout lay = make_search_layout(h->d, h->dtype, Lmax, h->Rp, 2 * Lmax + 64, false,
+                                      use_h24(h), false);
+  if ((size_t)lay.total > 227 * 1024)
     return fail(h, DD_ERR_UNSUPPORTED, "query shared memory %u B too large", lay.total);
-  const int bps = search_blocks_per_sm(view(h), lay, Lmax, wpc);
-  const int grid = (int)std::min<uint64_t>((nq + wpc - 1) / wpc, (uint64_t)bps * h->sm_count);
+  const LaunchPlan plan = plan_query(view(h), lay, Lmax);
+  const int wpc = plan.warps_per_cta;
+  const int grid = (int)std::min<uint64_t>((nq + wpc - 1) / wpc,
+                                           (uint64_t)plan.blocks_per_sm * h->sm_count);
   QueryArgs qa;
   qa.queries = (const uint8_t*)queries;
   qa.qstride = qstride;

@@ -38,7 +38,7 @@ static __host__ __device__ inline uint32_t r16(uint64_t x) {
 // With h24 the hash table stores 24-bit ids (3 bytes a slot instead of 4),
 // which is exact whenever every id is below 0xFFFFFF.
 WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, uint32_t vcap,
-                              bool build, bool h24) {
+                              bool build, bool h24, bool keep_vis) {
   WarpLayout w{};
   uint32_t esz = dtype == DD_F32 ? 4 : 1;
   uint32_t off = 0;
@@ -59,8 +59,11 @@ WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, ui
     w.ws = off;
     off += hash_bytes;
   } else {
-    w.vis_id = off; off += r16(4ull * vcap);
-    w.vis_d = off; off += r16(4ull * vcap);
+    w.keep_vis = keep_vis ? 1u : 0u;
+    if (keep_vis) {
+      w.vis_id = off; off += r16(4ull * vcap);
+      w.vis_d = off; off += r16(4ull * vcap);
+    }
     w.ws = off; off += r16(4ull * vcap);  // evicted list
     off += hash_bytes;
   }
@@ -111,8 +114,8 @@ __device__ __forceinline__ SearchSmem carve_query(uint8_t* base, const WarpLayou
   S.c_d = (float*)(base + w.c_d);
   S.s_id = (uint32_t*)(base + w.s_id);
   S.s_d = (float*)(base + w.s_d);
-  S.vis_id = (uint32_t*)(base + w.vis_id);
-  S.vis_d = (float*)(base + w.vis_d);
+  S.vis_id = w.keep_vis ? (uint32_t*)(base + w.vis_id) : nullptr;
+  S.vis_d = w.keep_vis ? (float*)(base + w.vis_d) : nullptr;
   S.ev_id = (uint32_t*)(base + w.ws);
   S.hash = (uint32_t*)(base + w.ws + r16(4ull * w.vcap));
   S.h24 = (int)w.h24;
@@ -512,7 +515,7 @@ __global__ void __launch_bounds__(kBigThreads) k_reverse_big(IndexView ix, Round
 
 // ============================================================ queries
 template <int DT, int MT, int FPL, int CPL>
-__global__ void __launch_bounds__(128) k_query(IndexView ix, QueryArgs qa, WarpLayout lay) {
+__global__ void __launch_bounds__(512) k_query(IndexView ix, QueryArgs qa, WarpLayout lay) {
   extern __shared__ uint4 smem_raw[];
   const uint32_t wpc = blockDim.x >> 5, wic = threadIdx.x >> 5, lane = lane_id();
   const uint64_t gw = (uint64_t)blockIdx.x * wpc + wic;
@@ -816,16 +819,6 @@ static int occupancy(K kernel, int threads, size_t smem) {
   return b > 0 ? b : 1;
 }
 
-int search_blocks_per_sm(const IndexView& ix, const WarpLayout& lay, uint32_t L, int wpc) {
-  size_t sm = (size_t)lay.total * wpc;
-  int b = 1;
-#define OCC4(DT, MT, F, C) b = occupancy(k_query<DT, MT, F, C>, wpc * 32, sm);
-#define OCC(DT, MT) DD_DISPATCH_FC(L, ix.Rp, DT, MT, OCC4)
-  DD_DISPATCH_DM(ix.dtype, ix.metric, OCC);
-#undef OCC
-#undef OCC4
-  return b;
-}
 
 // Warps per CTA of a per-warp kernel: the CTA size (up to 16 warps) that keeps
 // the most warps resident per SM, the smaller CTA on ties.
@@ -841,6 +834,16 @@ static LaunchPlan plan_warp_kernel(K kernel, uint32_t bytes_per_warp) {
   }
   if (best.blocks_per_sm == 0) best.blocks_per_sm = 1;
   return best;
+}
+
+LaunchPlan plan_query(const IndexView& ix, const WarpLayout& lay, uint32_t Lmax) {
+  LaunchPlan p{1, 1};
+#define CALL4(DT, MT, F, C) p = plan_warp_kernel(k_query<DT, MT, F, C>, lay.total);
+#define CALL(DT, MT) DD_DISPATCH_FC(Lmax, ix.Rp, DT, MT, CALL4)
+  DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
+#undef CALL
+#undef CALL4
+  return p;
 }
 
 LaunchPlan plan_search(const IndexView& ix, const WarpLayout& lay, uint32_t L) {

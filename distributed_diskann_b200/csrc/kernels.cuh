@@ -17,6 +17,7 @@ struct WarpLayout {
   uint32_t ccap;   // prune candidate capacity (visited list + out-list)
   uint32_t hbits;  // hash bits of the largest beam width of the launch
   uint32_t h24;    // hash table of 24-bit ids (every id < 0xFFFFFF)
+  uint32_t keep_vis;  // query layout holds the visited list (debug beam search)
 };
 
 // Per-warp shared-memory carve-up of k_prune (byte offsets, 16-byte aligned).
@@ -41,11 +42,12 @@ struct IndexView {
   uint32_t* err;
 };
 
+// keep_vis: the query layout reserves the visited list (k_beam keeps it;
+// k_query only needs the evicted list)
 WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, uint32_t vcap,
-                              bool build, bool h24);
+                              bool build, bool h24, bool keep_vis = true);
 PruneLayout make_prune_layout(uint32_t d, int dtype, uint32_t Rp, uint32_t ccap);
-// CTAs of k_query resident per SM for a layout
-int search_blocks_per_sm(const IndexView& ix, const WarpLayout& lay, uint32_t L, int wpc);
+
 
 struct RoundArgs {
   uint64_t floor;
@@ -113,6 +115,7 @@ struct QueryArgs {
   uint32_t* visited;       // nq (may be null)
   uint32_t* cmps;          // nq (may be null)
 };
+LaunchPlan plan_query(const IndexView& ix, const WarpLayout& lay, uint32_t Lmax);
 void launch_query(const IndexView& ix, const QueryArgs& qa, const WarpLayout& lay,
                   int warps_per_cta, int grid, cudaStream_t st);
 
