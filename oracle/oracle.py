@@ -189,8 +189,12 @@ def read_graph(path: str) -> np.ndarray:
     g = np.zeros((n, R + 1), dtype=np.uint32)
     g[:, 0] = deg
     off = np.concatenate([[0], np.cumsum(deg.astype(np.int64))])
-    for i in range(n):
-        g[i, 1 : 1 + deg[i]] = edges[off[i] : off[i + 1]]
+    for lo in range(0, n, 1 << 20):  # blocks of rows, vectorised inside a block
+        hi = min(n, lo + (1 << 20))
+        d = deg[lo:hi].astype(np.int64)
+        rows = np.repeat(np.arange(lo, hi), d)
+        cols = np.arange(off[hi] - off[lo]) - np.repeat(off[lo:hi] - off[lo], d) + 1
+        g[rows, cols] = edges[off[lo] : off[hi]]
     return g
 
 
