@@ -56,6 +56,7 @@ struct dd_index {
   uint64_t vis_all_words = 0;
   uint32_t* ref_rows = nullptr;  // n x (R+1) reference-layout rows for downloads
   bool verbose = false;
+  bool hash32 = false;  // DD_HASH32=1: 32-bit hash-table ids even when n < 2^24 - 1
 };
 
 namespace {
@@ -207,8 +208,9 @@ int ensure_vis_all(dd_index* h, uint64_t words) {
   return DD_OK;
 }
 
-// ids fit the 24-bit hash table layout
-bool use_h24(const dd_index* h) { return h->n < 0xFFFFFFull; }
+// ids fit the 24-bit hash table layout (DD_HASH32=1 at dd_create keeps the
+// 32-bit layout, which larger indexes use, for testing it on small data)
+bool use_h24(const dd_index* h) { return h->n < 0xFFFFFFull && !h->hash32; }
 
 // the reverse-edge scratch of a handle; `res` = semisort result buffer
 ReverseScratch make_rs(dd_index* h, int res) {
@@ -371,6 +373,8 @@ int dd_create(int dtype, int metric, uint64_t n, uint32_t d, uint32_t R, int dev
   {
     const char* v = getenv("DD_VERBOSE");
     h->verbose = v && v[0] == '1';
+    const char* w = getenv("DD_HASH32");
+    h->hash32 = w && w[0] == '1';
   }
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device);

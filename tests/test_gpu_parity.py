@@ -198,3 +198,21 @@ def test_error_word_reports_bad_graph_ids():
     with pytest.raises(DDError):
         gi.set_graph(bad)
     gi.close()
+
+
+def test_32bit_hash_table_layout_matches_24bit(monkeypatch):
+    """Indexes with n >= 2^24 - 1 keep the lossy filter's ids in 32 bits; here
+    DD_HASH32=1 selects that layout on small data.  Graph, search results and
+    the reference's visited / dist_cmps counters must equal the 24-bit layout's
+    (which the other tests check against the reference)."""
+    base = D.gen_mixture_i8(20_000, 48, 200, 7)
+    q = D.gen_mixture_i8(500, 48, 200, 8)
+    out = []
+    for flag in ("0", "1"):
+        monkeypatch.setenv("DD_HASH32", flag)
+        gi, graph, st = gpu_build(base, 32, 64, 1.2)
+        ids, _, vis, cm = gi.search(q, 10, [10, 50, 100, 200, 64] * 100)
+        out.append((graph, st["visited"], st["dist_cmps"], ids, vis, cm))
+        gi.close()
+    for a, b in zip(out[0], out[1]):
+        np.testing.assert_array_equal(a, b)
