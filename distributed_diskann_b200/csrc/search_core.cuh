@@ -222,6 +222,12 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
       uint32_t b = __ballot_sync(FULL, unv);
       if (b) { nxt_pos = (int)(base + __ffs(b) - 1); break; }
     }
+    // its row is brought into L2 now (128-byte lines, one per lane); the
+    // speculative load of the next row then usually hits L2
+    if (nxt_pos >= 0 && lane * 32u < dl) {
+      const uint32_t* nrow = P.graph + (uint64_t)S.fr_id[nxt_pos] * P.Rp + lane * 32u;
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(nrow));
+    }
 
     // ---- hash filter, replayed chunk by chunk in neighbour order.  The
     // slots, same-slot groups and predecessor ids of all chunks are computed
