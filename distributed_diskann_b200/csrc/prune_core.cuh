@@ -7,7 +7,8 @@
 //  2. greedy selection: walk the sorted list, skip p and removed entries,
 //     select p*, and remove every later p' with alpha * d(p*, p') <= d(p, p')
 //     (alpha is a double in the reference, so the test is done in double).
-//     The occlusion distances of one p* are spread over the 32 lanes.
+//     Three exact forms: INT8 tensor-core Gram tiles (integer data), rows in
+//     registers (float rows <= 256 bytes), and a per-lane form (the rest).
 #pragma once
 #include "dd_common.cuh"
 #include "sort_emul.cuh"
@@ -27,7 +28,7 @@ struct PruneSmem {
   int* stack;         // ddsort::stack_ints(capacity) ints
   int* posL;          // rank-pairing scratch, capacity ints each
   int* posR;
-  uint4* sel;         // selected rows of warp_greedy_select_reg (overlays posL/posR), or null
+  uint4* sel;         // rows of the register / tensor-core greedy (overlays posL/posR), or null
 };
 
 // bytes of the leaf bitmap + stack + rank scratch for `cap` candidates (16-byte multiple)
@@ -802,25 +803,6 @@ __device__ __forceinline__ void warp_sort_pairs(uint32_t* ids, float* keys, uint
             keys[i] = kl; keys[l] = ki;
             ids[i] = il; ids[l] = ii;
           }
-        }
-      }
-      __syncwarp();
-    }
-  }
-}
-
-// same network on plain uint32 keys (reverse-edge segments)
-__device__ __forceinline__ void warp_sort_u32(uint32_t* a, uint32_t n) {
-  const uint32_t lane = lane_id();
-  uint32_t N = 1;
-  while (N < n) N <<= 1;
-  for (uint32_t k = 2; k <= N; k <<= 1) {
-    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-      for (uint32_t i = lane; i < N; i += 32) {
-        uint32_t l = (j == (k >> 1)) ? (i ^ (k - 1)) : (i ^ j);
-        if (l > i && l < n) {
-          uint32_t x = a[i], y = a[l];
-          if (y < x) { a[i] = y; a[l] = x; }
         }
       }
       __syncwarp();

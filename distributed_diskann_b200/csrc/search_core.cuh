@@ -25,7 +25,7 @@
 //    slot are grouped with __match_any_sync; within a group the table value a
 //    lane sees is the id of the previous lane in neighbour order (or the table
 //    entry), and the last lane of the group writes the slot.  The table lives
-//    in a per-warp slice of global memory (L1/L2 resident).
+//    in the warp's shared memory (24-bit ids when every id is below 0xFFFFFF).
 //  * set_union + trim: candidates are ranked by (dist, id), the copies
 //    set_union adds are kept, and every element moves to its merged position;
 //    positions >= L are dropped.
