@@ -326,7 +326,10 @@ int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& r
     SemisortScratch ss = make_ss(h);
     const int res = launch_semisort(h->new_out, B * h->Rp, h->n, ss, h->stream);
     launch_reverse(ix, ra, make_rs(h, res), h->stream, h->sm_count);
-    h->launches += 7 + 5 * (uint64_t)((64 - __builtin_clzll(h->n > 1 ? h->n - 1 : 1) + 7) / 8);
+    // k_search, k_prune, k_apply_rows, k_reverse, k_reverse_big; per radix
+    // pass a histogram, three scans and a scatter; the segment heads' flags,
+    // three scans and scatter
+    h->launches += 10 + 5 * (uint64_t)((64 - __builtin_clzll(h->n > 1 ? h->n - 1 : 1) + 7) / 8);
     if (P->collect_stats) {
       k_accumulate<<<64, 256, 0, h->stream>>>(h->stat_vis, h->stat_cmps, (uint32_t)B, h->counters,
                                               h->acc);
