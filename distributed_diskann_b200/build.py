@@ -17,7 +17,8 @@ CSRC = os.path.join(PKG, "csrc")
 OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "libdd_gpu.so")
 OBJ_DIR = os.path.join(PKG, "_build")
-SOURCES = ["kernels.cu", "semisort.cu", "dd_api.cu", "noalloc.cu"]
+SOURCES = ["k_search.cu", "k_prune.cu", "k_reverse.cu", "k_misc.cu", "semisort.cu", "dd_api.cu",
+           "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
 

@@ -1,0 +1,83 @@
+// Helpers shared by the kernel translation units: sizes, vector loads,
+// dtype/metric dispatch and CTA-shape planning of one-warp-per-item kernels.
+#pragma once
+#include <algorithm>
+#include <cstdint>
+
+#include "dd_common.cuh"
+#include "kernels.cuh"
+
+namespace ddk {
+
+static __host__ __device__ inline uint32_t r16(uint64_t x) {
+  return (uint32_t)((x + 15) & ~(uint64_t)15);
+}
+
+// copy a padded vector row into shared memory (16-byte granules)
+__device__ __forceinline__ void load_vec(uint8_t* dst, const uint8_t* src, uint32_t bytes16) {
+  const uint4* s4 = (const uint4*)src;
+  uint4* d4 = (uint4*)dst;
+  for (uint32_t i = lane_id(); i < bytes16 / 16; i += 32) d4[i] = __ldg(s4 + i);
+}
+
+// number of valid neighbours (the valid entries are a prefix of the row)
+__device__ __forceinline__ uint32_t row_degree(const uint32_t* row, uint32_t Rp) {
+  uint32_t deg = 0;
+  for (uint32_t base = 0; base < Rp; base += 32) {
+    uint32_t j = base + lane_id();
+    bool v = (j < Rp) && (row[j] != DD_NONE);
+    deg += __popc(__ballot_sync(0xffffffffu, v));
+  }
+  return deg;
+}
+
+#define DD_DISPATCH_DM(dtype, metric, CALL)                                          \
+  do {                                                                               \
+    if ((dtype) == DD_F32 && (metric) == DD_L2) { CALL(DD_F32, DD_L2); }             \
+    else if ((dtype) == DD_F32) { CALL(DD_F32, DD_MIPS); }                           \
+    else if ((dtype) == DD_I8 && (metric) == DD_L2) { CALL(DD_I8, DD_L2); }          \
+    else if ((dtype) == DD_I8) { CALL(DD_I8, DD_MIPS); }                             \
+    else if ((metric) == DD_L2) { CALL(DD_U8, DD_L2); }                              \
+    else { CALL(DD_U8, DD_MIPS); }                                                   \
+  } while (0)
+
+// frontier / row register buckets: (L <= 128 | L <= 512) x (Rp <= 64 | Rp <= 128)
+#define DD_DISPATCH_FC(L, Rp, DT, MT, CALL4)                                         \
+  do {                                                                               \
+    if ((L) <= 128 && (Rp) <= 64) { CALL4(DT, MT, 4, 2); }                           \
+    else if ((L) <= 128) { CALL4(DT, MT, 4, 4); }                                    \
+    else if ((Rp) <= 64) { CALL4(DT, MT, 16, 2); }                                   \
+    else { CALL4(DT, MT, 16, 4); }                                                   \
+  } while (0)
+
+template <typename K>
+static void set_smem(K kernel, size_t bytes) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <typename K>
+static int occupancy(K kernel, int threads, size_t smem) {
+  set_smem(kernel, smem);
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, smem) != cudaSuccess) b = 1;
+  return b > 0 ? b : 1;
+}
+
+
+// Warps per CTA of a per-warp kernel: the CTA size (up to 16 warps) that keeps
+// the most warps resident per SM, the smaller CTA on ties.
+template <typename K>
+static LaunchPlan plan_warp_kernel(K kernel, uint32_t bytes_per_warp) {
+  LaunchPlan best{1, 0};
+  static const int cand[] = {1, 2, 4, 5, 8, 16};
+  for (int wpc : cand) {
+    const size_t sm = (size_t)bytes_per_warp * wpc;
+    if (sm > 227 * 1024) break;
+    const int b = occupancy(kernel, wpc * 32, sm);
+    if (b * wpc > best.warps_per_cta * best.blocks_per_sm) best = LaunchPlan{wpc, b};
+  }
+  if (best.blocks_per_sm == 0) best.blocks_per_sm = 1;
+  return best;
+}
+
+}  // namespace ddk

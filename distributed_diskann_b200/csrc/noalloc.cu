@@ -7,8 +7,8 @@
 // device and stall its other streams), or a caller whose memory belongs to
 // another allocator that must not be bypassed.  For them this entry point
 // takes device pointers for every input and output and keeps its candidate
-// workspace in the fixed-size device array below, which every GPU that loads the library holds until the
-// process exits.
+// workspace in the fixed-size device array below, which every GPU that loads
+// the library holds until the process exits.
 //
 // The workspace is shared by all calls on a device and keeps the last call's
 // contents.  Every call rewrites each part of it before reading it (the leaf
@@ -43,15 +43,23 @@ std::mutex g_mu;
 void* g_workspace_addr[256] = {nullptr};
 
 // k_prune_tasks with the workspace slices carved from the fixed array and with
-// the device-side inputs validated (the host cannot read them)
+// the device-side inputs validated (the host cannot read them).  Task slices
+// are disjoint only when the offsets never decrease, so every warp first checks
+// the whole offsets array (at most kNoAllocMaxTasks + 1 words): offsets that
+// decrease or do not end at `total` invalidate the call and every row is
+// padded.  An id >= n (p or a candidate) pads only its own task's row.
 template <int DT, int MT>
 __global__ void k_prune_tasks_fixed(IndexView ix, PruneArgs pa, uint64_t total) {
   const uint32_t lane = lane_id();
+  bool offsets_ok = pa.offsets[pa.ntasks] == total;
+  for (uint32_t t = lane; t < pa.ntasks; t += 32)
+    if (pa.offsets[t] > pa.offsets[t + 1]) offsets_ok = false;
+  offsets_ok = __all_sync(0xffffffffu, offsets_ok);
   for (uint32_t t = blockIdx.x; t < pa.ntasks; t += gridDim.x) {
     uint32_t* out_row = pa.out + (uint64_t)t * ix.Rp;
     const uint32_t p = pa.p[t];
     const uint64_t o0 = pa.offsets[t], o1 = pa.offsets[t + 1];
-    bool ok = p < ix.n && o0 <= o1 && o1 <= total;
+    bool ok = offsets_ok && p < ix.n;
     if (ok) {
       for (uint64_t j = o0 + lane; j < o1; j += 32)
         if (pa.cand_ids[j] >= ix.n) ok = false;

@@ -159,9 +159,11 @@ int dd_robust_prune(dd_index* h, uint32_t ntasks, const uint32_t* p, const uint6
  * device address; make it before any stream capture.  All calls on a device
  * share the array: calls whose kernels overlap on the GPU race and must be
  * serialized.  The kernel runs on the handle's stream; with synchronize != 0
- * the call waits for it and reports invalid device inputs (ids >= n, bad
- * offsets), otherwise those rows are left as padding and the handle's error
- * word reports them at its next synchronizing call. */
+ * the call waits for it and reports invalid device inputs as DD_ERR_DEVICE,
+ * otherwise the handle's error word reports them at its next synchronizing
+ * call.  Offsets that decrease or do not end at total_cands invalidate the
+ * whole call (every row is padding); an id >= n (p[t] or a candidate of task
+ * t) pads only row t.  Rows of valid tasks are correct in both cases. */
 int dd_robust_prune_noalloc(dd_index* h, uint32_t ntasks, const uint32_t* p,
                             const uint64_t* offsets, uint64_t total_cands,
                             const uint32_t* cand_ids, const float* cand_dists, double alpha,

@@ -18,6 +18,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libdd_oracle.so")
 REF_HARNESS = os.path.join(HERE, "_ref", "ref_harness")
+# where the reference tree lies (only the machine that builds the harness has it)
+REF_ROOT = os.environ.get("DD_REFERENCE_ROOT", "/root/reference")
 
 DTYPES = {np.dtype(np.float32): 0, np.dtype(np.int8): 1, np.dtype(np.uint8): 2}
 DTYPE_NAMES = {0: "f32", 1: "i8", 2: "u8"}
@@ -30,7 +32,7 @@ def build_oracle() -> None:
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
 
 
-def build_reference(ref_root: str = "/root/reference") -> bool:
+def build_reference(ref_root: str = REF_ROOT) -> bool:
     """Compile the reference harness if its sources are present (this container)."""
     if os.path.exists(REF_HARNESS):
         return True
@@ -263,6 +265,33 @@ def ref_search(points, graph, queries, k, L, cut=1.35, metric="l2", start=0, lim
         # entries past the final frontier are undefined in the reference: mask them
         ids[np.arange(k)[None, :] >= fsz[:, None]] = 0xFFFFFFFF
         return ids, vis, cmps, _parse_seconds(out, "HARNESS_SEARCH_SECONDS")
+
+
+def ref_qps(points, graph, queries, k, Ls, cut=1.35, metric="l2", start=0, threads=0):
+    """The reference's searchAll timed like checkRecall (untimed pass, then a
+    timed one) for each beam width in Ls, on one loaded index.  Returns
+    {L: (ids nq x k, seconds)}; ids past a short final frontier are undefined
+    in the reference and are not masked here."""
+    points = np.ascontiguousarray(points)
+    dt = DTYPE_NAMES[DTYPES[points.dtype]]
+    nq = queries.shape[0]
+    with tempfile.TemporaryDirectory() as td:
+        base, qf, gf, of = (os.path.join(td, x) for x in ("b.bin", "q.bin", "g.bin", "o.bin"))
+        write_bin(base, points)
+        write_bin(qf, np.ascontiguousarray(queries, dtype=points.dtype))
+        write_graph(gf, graph)
+        out = _run_ref(["qps", dt, metric, base, gf, qf, k, cut, start,
+                        ",".join(str(int(L)) for L in Ls), of], threads)
+        raw = np.fromfile(of, dtype=np.uint32)
+    secs = {}
+    for line in out.splitlines():
+        if line.startswith("HARNESS_QPS"):
+            _, L, s = line.split()
+            secs[int(L)] = float(s)
+    res = {}
+    for i, L in enumerate(Ls):
+        res[int(L)] = (raw[i * nq * k : (i + 1) * nq * k].reshape(nq, k).copy(), secs[int(L)])
+    return res
 
 
 def ref_beam(points, graph, queries, k, L, cut=0.0, metric="l2", start=0, limit=0,

@@ -10,6 +10,7 @@
 //   knnbuild: knn_index<...>::build_index (include/index.h:125-137), the -DORIGINAL_PARLAY path
 //   search  : searchAll (include/utils/beamSearch.h:314-346), timed twice like
 //             checkRecall (include/utils/check_nn_recall.h:62-66)
+//   qps     : the same timing for a list of beam widths on one loaded index
 //   beam    : beam_search (include/utils/beamSearch.h:51-184), full frontier + visited
 //   prune   : knn_index::robustPrune (include/index.h:63-123)
 //
@@ -104,6 +105,41 @@ int run(int argc, char** argv) {
     double t1 = now_s();
     std::printf("HARNESS_BUILD_SECONDS %.9f\n", t1 - t0);
     G.save(argv[9]);
+    return 0;
+  }
+  if (cmd == "qps") {
+    // qps <dtype> <metric> <base> <graph> <queries> <k> <cut> <start> <L1,L2,...> <out>
+    // checkRecall's timing (include/utils/check_nn_recall.h:62-66) for each beam
+    // width: searchAll once untimed, then once timed; ids of the timed pass out
+    if (argc < 12) die("qps: bad args");
+    Graph<unsigned int> G(argv[5]);
+    PR Q(argv[6]);
+    long k = std::atol(argv[7]);
+    double cut = std::atof(argv[8]);
+    idx_t start = (idx_t)std::atol(argv[9]);
+    FILE* out = std::fopen(argv[11], "wb");
+    if (!out) die("cannot open output");
+    std::string Ls = argv[10];
+    size_t pos = 0;
+    while (pos < Ls.size()) {
+      size_t e = Ls.find(',', pos);
+      if (e == std::string::npos) e = Ls.size();
+      long L = std::atol(Ls.substr(pos, e - pos).c_str());
+      pos = e + 1;
+      QueryParams QP(k, L, cut, (long)G.size(), G.max_degree());
+      stats<unsigned int> QS(Q.size());
+      auto r1 = searchAll<Point, PR, unsigned int>(Q, G, Points, QS, start, QP);
+      QS.clear();
+      double t0 = now_s();
+      auto r2 = searchAll<Point, PR, unsigned int>(Q, G, Points, QS, start, QP);
+      double t1 = now_s();
+      std::printf("HARNESS_QPS %ld %.9f\n", L, t1 - t0);
+      std::vector<uint32_t> ids;
+      for (size_t i = 0; i < Q.size(); i++)
+        for (long j = 0; j < k; j++) ids.push_back(r2[i][j]);
+      write_u32(out, ids);
+    }
+    std::fclose(out);
     return 0;
   }
   if (cmd == "search" || cmd == "beam") {

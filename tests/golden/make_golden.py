@@ -33,7 +33,7 @@ from distributed_diskann_b200 import datasets as D  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
 OUT_DIR = os.path.dirname(os.path.abspath(__file__))
-REF_DATA = "/root/reference/data/random10000"
+REF_DATA = os.path.join(O.REF_ROOT, "data", "random10000")
 
 
 def sha(a) -> str:
