@@ -13,6 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libdd_gpu.so")
 
 DD_OK = 0
+MODES = {"fast": 0, "plain": 1}
 ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "out of device memory",
           4: "device error word", 5: "unsupported parameter", 6: "I/O error"}
 
@@ -28,14 +29,16 @@ class DDError(RuntimeError):
 class BuildParamsC(C.Structure):
     _fields_ = [("L", u32), ("alpha", dbl), ("max_fraction", dbl), ("max_build", u64),
                 ("start_point", u32), ("two_pass", C.c_int32), ("knn_mode", C.c_int32),
-                ("collect_stats", C.c_int32), ("vcap", u32)]
+                ("collect_stats", C.c_int32), ("vcap", u32), ("mode", C.c_int32)]
 
 
 class StatsC(C.Structure):
     _fields_ = [("rounds", u64), ("visited", u64), ("dist_cmps", u64), ("groups", u64),
                 ("reverse_prunes", u64), ("prune_cands", u64), ("big_groups", u64),
                 ("build_ms", dbl), ("search_prune_ms", dbl), ("reverse_ms", dbl),
-                ("search_ms", dbl)]
+                ("search_ms", dbl), ("search_warps_per_cta", u32), ("prune_warps_per_cta", u32),
+                ("search_queue", C.c_int32), ("prune_queue", C.c_int32),
+                ("graph_replay", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -48,6 +51,8 @@ SIGNATURES = {
     "dd_destroy": (i32, [vp]),
     "dd_last_error": (C.c_char_p, [vp]),
     "dd_set_stream": (i32, [vp, vp]),
+    "dd_set_search_mode": (i32, [vp, i32]),
+    "dd_check_errors": (i32, [vp]),
     "dd_upload_points": (i32, [vp, vp, u64]),
     "dd_upload_points_device": (i32, [vp, vp, u64]),
     "dd_load_points_file": (i32, [vp, C.c_char_p]),

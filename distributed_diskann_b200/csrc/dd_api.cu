@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -57,6 +58,18 @@ struct dd_index {
   uint32_t* ref_rows = nullptr;  // n x (R+1) reference-layout rows for downloads
   bool verbose = false;
   bool hash32 = false;  // DD_HASH32=1: 32-bit hash-table ids even when n < 2^24 - 1
+  int search_mode = DD_MODE_FAST;
+  // fast form: device work queues (two per round and pass), the CUDA graph of
+  // the last build sequence and the stream it is captured on
+  uint32_t* queues = nullptr;
+  uint64_t queue_words = 0;
+  uint64_t scratch_gen = 0;  // bumped whenever build scratch is reallocated
+  cudaStream_t own_stream = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  uint64_t launches_per_graph = 0;
+  uint32_t* qcls = nullptr;  // query class lists, counts and queues (fast search form)
+  uint64_t qcls_words = 0;
+  std::vector<uint64_t> graph_key;  // what the captured graph was built for
 };
 
 namespace {
@@ -156,6 +169,7 @@ int ensure_build_scratch(dd_index* h, uint64_t B) {
     CK(dalloc(&h->acc, 8));
   }
   if (B <= h->bcap) return DD_OK;
+  h->scratch_gen++;
   void* old[] = {h->new_out, h->stat_vis, h->stat_cmps, h->sort_t[0], h->sort_t[1], h->sort_v[0],
                  h->sort_v[1], h->hist, h->heads, h->flags, h->big, h->gcand, h->gkey,
                  h->gpos, h->gbits, h->granges};
@@ -200,11 +214,24 @@ SemisortScratch make_ss(dd_index* h) {
 // room for `words` uint32 of per-point visited lists
 int ensure_vis_all(dd_index* h, uint64_t words) {
   if (words <= h->vis_all_words) return DD_OK;
+  h->scratch_gen++;
   dfree(h->vis_all);
   h->vis_all = nullptr;
   h->vis_all_words = 0;
   CK(dalloc(&h->vis_all, words));
   h->vis_all_words = words;
+  return DD_OK;
+}
+
+// room for `words` work-queue counters
+int ensure_queues(dd_index* h, uint64_t words) {
+  if (words <= h->queue_words) return DD_OK;
+  h->scratch_gen++;
+  dfree(h->queues);
+  h->queues = nullptr;
+  h->queue_words = 0;
+  CK(dalloc(&h->queues, words));
+  h->queue_words = words;
   return DD_OK;
 }
 
@@ -288,12 +315,135 @@ struct BuildPlan {
   LaunchPlan splan;
   PruneLayout play;
   LaunchPlan pplan;
+  bool fast;     // DD_MODE_FAST: tensor-core greedy of robustPrune (integer data)
+  bool squeue;   // persistent k_search fed by the round's work queue
+  bool pqueue;   // persistent k_prune fed by the round's work queue
 };
 
-int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& rounds, double alpha,
-                const dd_build_params* P, const BuildPlan& bp, PhaseEvents* pe) {
+// ---------------------------------------------------------------- autotuner
+// The fast form's CTA shapes are picked by timing: at the first round of a
+// build with at least kTuneItems points, k_search and k_prune are run on the
+// round's first kTuneItems points with every candidate shape (2/4/8/16 warps
+// per CTA, with and without the device work queue) and the fastest is kept
+// for the rest of the build and for later builds of the same shape.  Both
+// kernels only write scratch (visited lists, new out-lists) that the real
+// launch of the round then rewrites, so the calibration does not change the
+// build.  Results are cached per process, keyed by the shape.
+constexpr uint32_t kTuneItems = 32768;
+
+struct TuneResult {
+  LaunchPlan splan, pplan;
+  bool squeue = true, pqueue = true;
+  float search_ms = 0.f, prune_ms = 0.f;  // calibration time of the chosen shapes
+};
+
+std::mutex g_tune_mu;
+std::vector<std::pair<std::vector<uint64_t>, TuneResult>> g_tune;
+
+std::vector<uint64_t> tune_key(const dd_index* h, const BuildPlan& bp, uint32_t L) {
+  return {(uint64_t)h->dtype, (uint64_t)h->metric, h->d, h->Rp, L, bp.slay.vcap, bp.slay.h24,
+          (uint64_t)bp.fast, (uint64_t)h->device};
+}
+
+bool tune_lookup(const std::vector<uint64_t>& key, TuneResult* out) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  for (auto& e : g_tune)
+    if (e.first == key) {
+      *out = e.second;
+      return true;
+    }
+  return false;
+}
+
+void tune_store(const std::vector<uint64_t>& key, const TuneResult& r) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  for (auto& e : g_tune)
+    if (e.first == key) {
+      e.second = r;
+      return;
+    }
+  g_tune.push_back({key, r});
+}
+
+int grid_for(const LaunchPlan& pl, uint64_t B, int sm_count) {
+  const uint64_t wpc = (uint64_t)pl.warps_per_cta;
+  return (int)std::min<uint64_t>((B + wpc - 1) / wpc, (uint64_t)pl.blocks_per_sm * sm_count);
+}
+
+// Times k_search and then k_prune of round `ra` (its first kTuneItems points)
+// for every candidate shape; the work-queue counter used is queues[0].
+int tune_round(dd_index* h, RoundArgs ra, BuildPlan* bp, TuneResult* res) {
   IndexView ix = view(h);
-  for (auto& rd : rounds) {
+  ra.B = std::min<uint32_t>(ra.B, kTuneItems);
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  auto timed = [&](auto&& launch, float* ms) -> int {
+    CK(cudaMemsetAsync(h->queues, 0, 4, h->stream));
+    CK(cudaEventRecord(a, h->stream));
+    launch();
+    CK(cudaEventRecord(b, h->stream));
+    CK(cudaEventSynchronize(b));
+    CK(cudaGetLastError());
+    CK(cudaEventElapsedTime(ms, a, b));
+    return DD_OK;
+  };
+  float best = 1e30f;
+  for (const LaunchPlan& pl : search_plan_candidates(ix, bp->slay, ra.L)) {
+    for (int q = 0; q < 2; q++) {
+      RoundArgs r2 = ra;
+      r2.qsearch = q ? h->queues : nullptr;
+      float ms = 0;
+      int rc = timed([&] { launch_search(ix, r2, bp->slay, pl, grid_for(pl, r2.B, h->sm_count),
+                                         h->stream); }, &ms);
+      if (rc) return rc;
+      if (ms < best) {
+        best = ms;
+        res->splan = pl;
+        res->squeue = q != 0;
+        res->search_ms = ms;
+      }
+    }
+  }
+  best = 1e30f;
+  for (const LaunchPlan& pl : prune_plan_candidates(ix, bp->play, bp->fast)) {
+    for (int q = 0; q < 2; q++) {
+      RoundArgs r2 = ra;
+      r2.qprune = q ? h->queues : nullptr;
+      float ms = 0;
+      int rc = timed([&] { launch_prune_round(ix, r2, bp->play, bp->slay.vcap, pl,
+                                              grid_for(pl, r2.B, h->sm_count), bp->fast,
+                                              h->stream); }, &ms);
+      if (rc) return rc;
+      if (ms < best) {
+        best = ms;
+        res->pplan = pl;
+        res->pqueue = q != 0;
+        res->prune_ms = ms;
+      }
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  bp->splan = res->splan;
+  bp->squeue = res->squeue;
+  bp->pplan = res->pplan;
+  bp->pqueue = res->pqueue;
+  return DD_OK;
+}
+
+// One pass of batch insertions (src/bsp_index.hpp:238-407) as stream-ordered
+// work with no host synchronization, so that a build can be captured in a
+// CUDA graph.  Round r of this pass uses work-queue counters
+// queues[qbase + 2r] (search) and [qbase + 2r + 1] (prune), zeroed by the
+// caller.  With `tune` set, the first round large enough is calibrated first
+// (tune_round), which synchronizes.
+int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& rounds, double alpha,
+                const dd_build_params* P, BuildPlan& bp, uint64_t qbase, PhaseEvents* pe,
+                TuneResult* tune) {
+  IndexView ix = view(h);
+  for (size_t r = 0; r < rounds.size(); r++) {
+    const auto& rd = rounds[r];
     uint64_t B = rd.second > rd.first ? rd.second - rd.first : 0;
     if (!B) continue;
     RoundArgs ra;
@@ -306,26 +456,26 @@ int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& r
     ra.stat_vis = h->stat_vis;
     ra.stat_cmps = h->stat_cmps;
     ra.vis_all = h->vis_all;
+    ra.qsearch = nullptr;
+    ra.qprune = nullptr;
+    if (tune && B >= kTuneItems) {
+      int rc = tune_round(h, ra, &bp, tune);
+      if (rc) return rc;
+      tune = nullptr;
+    }
+    if (bp.fast && bp.squeue) ra.qsearch = h->queues + qbase + 2 * r;
+    if (bp.fast && bp.pqueue) ra.qprune = h->queues + qbase + 2 * r + 1;
     CK(cudaMemsetAsync(h->counters, 0, 8 * 4, h->stream));
     if (pe) CK(cudaEventRecord(pe->next(), h->stream));
-    {
-      const uint64_t wpc = (uint64_t)bp.splan.warps_per_cta;
-      const int grid = (int)std::min<uint64_t>(
-          (B + wpc - 1) / wpc, (uint64_t)bp.splan.blocks_per_sm * h->sm_count);
-      launch_search(ix, ra, bp.slay, bp.splan, grid, h->stream);
-    }
+    launch_search(ix, ra, bp.slay, bp.splan, grid_for(bp.splan, B, h->sm_count), h->stream);
     if (pe) CK(cudaEventRecord(pe->next(), h->stream));
-    {
-      const uint64_t wpc = (uint64_t)bp.pplan.warps_per_cta;
-      const int grid = (int)std::min<uint64_t>(
-          (B + wpc - 1) / wpc, (uint64_t)bp.pplan.blocks_per_sm * h->sm_count);
-      launch_prune_round(ix, ra, bp.play, bp.slay.vcap, bp.pplan, grid, h->stream);
-    }
+    launch_prune_round(ix, ra, bp.play, bp.slay.vcap, bp.pplan,
+                       grid_for(bp.pplan, B, h->sm_count), bp.fast, h->stream);
     if (pe) CK(cudaEventRecord(pe->next(), h->stream));
     launch_apply_rows(ix, ra, h->stream);
     SemisortScratch ss = make_ss(h);
     const int res = launch_semisort(h->new_out, B * h->Rp, h->n, ss, h->stream);
-    launch_reverse(ix, ra, make_rs(h, res), h->stream, h->sm_count);
+    launch_reverse(ix, ra, make_rs(h, res), bp.fast, h->stream, h->sm_count);
     // k_search, k_prune, k_apply_rows, k_reverse, k_reverse_big; per radix
     // pass a histogram, three scans and a scatter; the segment heads' flags,
     // three scans and scatter
@@ -347,6 +497,30 @@ int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& r
               (unsigned long long)rd.first, (unsigned long long)rd.second, (unsigned long long)B,
               c[0], c[1], c[2], c[3], c[4], c[5]);
     }
+  }
+  return DD_OK;
+}
+
+// The whole device sequence of one build: reset, both passes, final sort.
+int build_sequence(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& rounds,
+                   const dd_build_params* Q, BuildPlan& bp, PhaseEvents* pe, TuneResult* tune) {
+  // empty graph (the reference starts from Graph(R, n): all degrees 0)
+  CK(cudaMemsetAsync(h->graph, 0xff, h->n * h->Rp * 4ull, h->stream));
+  CK(cudaMemsetAsync(h->acc, 0, 8 * 8, h->stream));
+  CK(cudaMemsetAsync(h->err, 0, 4, h->stream));
+  if (bp.fast) CK(cudaMemsetAsync(h->queues, 0, h->queue_words * 4, h->stream));
+  const uint64_t per_pass = 2 * rounds.size();
+  int rc;
+  if (Q->two_pass) {
+    rc = pass_rounds(h, rounds, 1.0, Q, bp, 2, pe, tune);
+    if (rc) return rc;
+    tune = nullptr;
+  }
+  rc = pass_rounds(h, rounds, Q->alpha, Q, bp, 2 + (Q->two_pass ? per_pass : 0), pe, tune);
+  if (rc) return rc;
+  if (Q->knn_mode) {
+    launch_sort_rows(view(h), h->stream);
+    h->launches++;
   }
   return DD_OK;
 }
@@ -405,6 +579,10 @@ int dd_destroy(dd_index* h) {
                   h->flags, h->counters, h->big, h->block_sums, h->acc, h->gcand, h->gkey,
                   h->gpos, h->gbits, h->granges, h->vis_all, h->ref_rows};
   for (void* p : ptrs) dfree(p);
+  dfree(h->queues);
+  dfree(h->qcls);
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
   return DD_OK;
 }
@@ -415,6 +593,20 @@ int dd_set_stream(dd_index* h, void* stream) {
   if (!h) return DD_ERR_ARG;
   h->stream = (cudaStream_t)stream;
   return DD_OK;
+}
+
+int dd_set_search_mode(dd_index* h, int mode) {
+  if (!h) return DD_ERR_ARG;
+  if (mode != DD_MODE_FAST && mode != DD_MODE_PLAIN)
+    return fail(h, DD_ERR_ARG, "mode must be DD_MODE_FAST or DD_MODE_PLAIN");
+  h->search_mode = mode;
+  return DD_OK;
+}
+
+int dd_check_errors(dd_index* h) {
+  if (!h) return DD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  return check_error_word(h);
 }
 
 int dd_upload_points(dd_index* h, const void* rows, uint64_t row_stride_bytes) {
@@ -538,6 +730,8 @@ int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
   uint32_t start = P->knn_mode ? 0 : P->start_point;  // include/index.h:127
   if (start >= h->n) return fail(h, DD_ERR_ARG, "start point %u >= n", start);
   if (!(P->alpha > 0)) return fail(h, DD_ERR_ARG, "alpha must be positive");
+  if (P->mode != DD_MODE_FAST && P->mode != DD_MODE_PLAIN)
+    return fail(h, DD_ERR_ARG, "mode must be DD_MODE_FAST or DD_MODE_PLAIN");
   CK(cudaSetDevice(h->device));
   h->launches = 0;
   auto rounds = schedule(h->n, P->max_build, P->max_fraction, P->knn_mode);
@@ -551,44 +745,97 @@ int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
   if (bp.slay.total > 227 * 1024)
     return fail(h, DD_ERR_UNSUPPORTED, "per-warp shared memory %u B too large (L=%u)",
                 bp.slay.total, P->L);
-  bp.play = make_prune_layout(h->d, h->dtype, h->Rp, bp.slay.ccap);
+  bp.fast = P->mode == DD_MODE_FAST;
+  bp.play = make_prune_layout(h->d, h->dtype, h->Rp, bp.slay.ccap, bp.fast);
   if (bp.play.total > 227 * 1024)
     return fail(h, DD_ERR_UNSUPPORTED, "prune shared memory %u B too large (visited capacity %u)",
                 bp.play.total, vcap);
   bp.splan = plan_search(view(h), bp.slay, P->L);
-  bp.pplan = plan_prune(view(h), bp.play);
+  bp.pplan = plan_prune(view(h), bp.play, bp.fast);
+  bp.squeue = bp.pqueue = bp.fast;
   rc = ensure_vis_all(h, Bmax * 2ull * vcap);
   if (rc) return rc;
+  rc = ensure_queues(h, 2 + 2 * rounds.size() * (P->two_pass ? 2 : 1));
+  if (rc) return rc;
 
-  // empty graph (the reference starts from Graph(R, n): all degrees 0)
-  CK(cudaMemsetAsync(h->graph, 0xff, h->n * h->Rp * 4ull, h->stream));
-  CK(cudaMemsetAsync(h->acc, 0, 8 * 8, h->stream));
-  CK(cudaMemsetAsync(h->err, 0, 4, h->stream));
+  // fast form: shapes from the autotuner's cache, or calibrated in this build
+  TuneResult tuned;
+  TuneResult* tune = nullptr;
+  const std::vector<uint64_t> tkey = tune_key(h, bp, P->L);
+  if (bp.fast) {
+    if (tune_lookup(tkey, &tuned)) {
+      bp.splan = tuned.splan;
+      bp.squeue = tuned.squeue;
+      bp.pplan = tuned.pplan;
+      bp.pqueue = tuned.pqueue;
+    } else if (Bmax >= kTuneItems) {
+      tune = &tuned;
+    }
+  }
+  dd_build_params Q = *P;
+  Q.start_point = start;
+  // A fast build with a settled shape and no statistics runs as one CUDA graph:
+  // captured once on the handle's private stream, replayed on later builds.
+  const bool use_graph = bp.fast && !tune && !P->collect_stats && !h->verbose;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   PhaseEvents pe;
-  PhaseEvents* pep = stats ? &pe : nullptr;
-  CK(cudaEventRecord(e0, h->stream));
-  float ts = 0, tp = 0, tr = 0;
-  dd_build_params Q = *P;
-  Q.start_point = start;
-  if (P->two_pass) {
-    rc = pass_rounds(h, rounds, 1.0, &Q, bp, pep);
+  PhaseEvents* pep = stats && P->collect_stats ? &pe : nullptr;
+  if (use_graph) {
+    std::vector<uint64_t> key = tkey;
+    uint64_t ab, mf;
+    std::memcpy(&ab, &P->alpha, 8);
+    std::memcpy(&mf, &P->max_fraction, 8);
+    key.insert(key.end(), {ab, mf, P->max_build, start, (uint64_t)P->two_pass,
+                           (uint64_t)P->knn_mode, h->scratch_gen,
+                           (uint64_t)bp.splan.warps_per_cta, (uint64_t)bp.splan.blocks_per_sm,
+                           (uint64_t)bp.pplan.warps_per_cta, (uint64_t)bp.pplan.blocks_per_sm,
+                           (uint64_t)bp.squeue, (uint64_t)bp.pqueue});
+    if (!h->gexec || h->graph_key != key) {
+      if (h->gexec) {
+        cudaGraphExecDestroy(h->gexec);
+        h->gexec = nullptr;
+      }
+      if (!h->own_stream) CK(cudaStreamCreate(&h->own_stream));
+      cudaStream_t user = h->stream;
+      h->stream = h->own_stream;
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeRelaxed));
+      rc = build_sequence(h, rounds, &Q, bp, nullptr, nullptr);
+      cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
+      h->stream = user;
+      if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      CK(ce);
+      cudaError_t ie = cudaGraphInstantiate(&h->gexec, g, 0);
+      cudaGraphDestroy(g);
+      if (ie != cudaSuccess) {
+        h->gexec = nullptr;
+        CK(ie);
+      }
+      h->graph_key = key;
+      h->launches_per_graph = h->launches;
+    }
+    h->launches = h->launches_per_graph;
+    cudaStream_t ls = h->stream ? h->stream : h->own_stream;
+    CK(cudaEventRecord(e0, ls));
+    CK(cudaGraphLaunch(h->gexec, ls));
+    CK(cudaEventRecord(e1, ls));
+  } else {
+    CK(cudaEventRecord(e0, h->stream));
+    rc = build_sequence(h, rounds, &Q, bp, pep, tune);
     if (rc) return rc;
+    CK(cudaEventRecord(e1, h->stream));
+    if (tune) tune_store(tkey, tuned);
   }
-  rc = pass_rounds(h, rounds, P->alpha, &Q, bp, pep);
-  if (rc) return rc;
-  if (P->knn_mode) {
-    launch_sort_rows(view(h), h->stream);
-    h->launches++;
-  }
-  CK(cudaEventRecord(e1, h->stream));
   CK(cudaEventSynchronize(e1));
   CK(cudaGetLastError());
   rc = check_error_word(h);
   if (stats) {
-    float ms = 0;
+    float ms = 0, ts = 0, tp = 0, tr = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     pe.sum(&ts, &tp, &tr);
     unsigned long long acc[8] = {0};
@@ -605,6 +852,11 @@ int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
     stats->search_prune_ms = ts + tp;
     stats->reverse_ms = tr;
     stats->search_ms = ts;
+    stats->search_warps_per_cta = (uint32_t)bp.splan.warps_per_cta;
+    stats->prune_warps_per_cta = (uint32_t)bp.pplan.warps_per_cta;
+    stats->search_queue = bp.fast && bp.squeue;
+    stats->prune_queue = bp.fast && bp.pqueue;
+    stats->graph_replay = use_graph;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -627,10 +879,6 @@ int dd_search_device(dd_index* h, const void* queries, uint64_t nq, uint64_t qst
                                       use_h24(h), false);
   if ((size_t)lay.total > 227 * 1024)
     return fail(h, DD_ERR_UNSUPPORTED, "query shared memory %u B too large", lay.total);
-  const LaunchPlan plan = plan_query(view(h), lay, Lmax);
-  const int wpc = plan.warps_per_cta;
-  const int grid = (int)std::min<uint64_t>((nq + wpc - 1) / wpc,
-                                           (uint64_t)plan.blocks_per_sm * h->sm_count);
   QueryArgs qa;
   qa.queries = (const uint8_t*)queries;
   qa.qstride = qstride;
@@ -647,8 +895,55 @@ int dd_search_device(dd_index* h, const void* queries, uint64_t nq, uint64_t qst
   qa.dists = dists;
   qa.visited = visited;
   qa.cmps = cmps;
-  launch_query(view(h), qa, lay, wpc, grid, h->stream);
+  qa.cls_items = nullptr;
+  qa.cls_count = nullptr;
+  qa.cls_queue = nullptr;
+  qa.Lvalid = Lmax;
+  if (h->search_mode == DD_MODE_PLAIN) {
+    // one launch laid out for the largest beam width
+    const LaunchPlan plan = plan_query(view(h), lay, Lmax);
+    const int wpc = plan.warps_per_cta;
+    const int grid = (int)std::min<uint64_t>((nq + wpc - 1) / wpc,
+                                             (uint64_t)plan.blocks_per_sm * h->sm_count);
+    launch_query(view(h), qa, lay, wpc, grid, h->stream);
+    h->launches = 1;
+    CK(cudaGetLastError());
+    return DD_OK;
+  }
+  // fast form: the queries are listed by beam-width class on the device, then
+  // each class runs as a persistent launch laid out for its own beam width
+  // (smaller hash table and frontier: more resident queries per SM), largest
+  // class first; classes without queries end at once
+  const uint64_t words = (uint64_t)kQueryClasses * nq + 2 * kQueryClasses;
+  if (words > h->qcls_words) {
+    dfree(h->qcls);
+    h->qcls = nullptr;
+    h->qcls_words = 0;
+    CK(dalloc(&h->qcls, words));
+    h->qcls_words = words;
+  }
+  uint32_t* counts = h->qcls + (uint64_t)kQueryClasses * nq;
+  uint32_t* queues = counts + kQueryClasses;
+  CK(cudaMemsetAsync(counts, 0, 2 * kQueryClasses * 4, h->stream));
+  launch_bin_queries(L_per_query, nq, k, Lmax, h->qcls, counts, h->stream);
   h->launches = 1;
+  for (int c = query_class(Lmax); c >= 0; c--) {
+    if ((16u << c) < k && c < query_class(Lmax)) break;  // no valid beam width below k
+    const uint32_t Lc = std::min<uint32_t>(16u << c, Lmax);
+    WarpLayout lc = make_search_layout(h->d, h->dtype, Lc, h->Rp, 2 * Lc + 64, false,
+                                       use_h24(h), false);
+    const LaunchPlan plan = plan_query(view(h), lc, Lc);
+    QueryArgs qc = qa;
+    qc.Lmax = Lc;
+    qc.cls_items = h->qcls + (uint64_t)c * nq;
+    qc.cls_count = counts + c;
+    qc.cls_queue = queues + c;
+    const int wpc = plan.warps_per_cta;
+    const int grid = (int)std::min<uint64_t>((nq + wpc - 1) / wpc,
+                                             (uint64_t)plan.blocks_per_sm * h->sm_count);
+    launch_query(view(h), qc, lc, wpc, grid, h->stream);
+    h->launches++;
+  }
   CK(cudaGetLastError());
   return DD_OK;
 }

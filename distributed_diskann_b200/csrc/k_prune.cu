@@ -19,14 +19,14 @@ namespace ddk {
 
 // Per-warp shared memory of k_prune: p's vector | candidate ids | distances |
 // sort workspace, which the fast greedy forms share after the sort.
-PruneLayout make_prune_layout(uint32_t d, int dtype, uint32_t Rp, uint32_t ccap) {
+PruneLayout make_prune_layout(uint32_t d, int dtype, uint32_t Rp, uint32_t ccap, bool tensor) {
   PruneLayout w{};
   uint32_t esz = dtype == DD_F32 ? 4 : 1;
   uint32_t off = 0;
   w.qv = off; off += r16((uint64_t)d * esz);
   w.cid = off; off += r16(4ull * ccap);
   w.ckey = off; off += r16(4ull * ccap);
-  w.ws = off; off += prune_ws_bytes_sel(ccap, greedy_sel_bytes(d, dtype, Rp));
+  w.ws = off; off += prune_ws_bytes_sel(ccap, greedy_sel_bytes(d, dtype, Rp, tensor));
   w.ccap = ccap;
   w.total = r16(off);
   return w;
@@ -34,7 +34,9 @@ PruneLayout make_prune_layout(uint32_t d, int dtype, uint32_t Rp, uint32_t ccap)
 
 // k_prune: one warp per batch point runs robustPrune of its visited list plus
 // its current out-list (include/index.h:279-285; src/bsp_index.hpp:269-277).
-template <int DT, int MT>
+// TC: occlusion distances from tensor-core Gram tiles where they apply (the
+// fast form); otherwise all on the CUDA cores (the plain form).
+template <int DT, int MT, bool TC>
 __global__ void __launch_bounds__(512) k_prune(IndexView ix, RoundArgs ra, PruneLayout lay,
                                                uint32_t vcap) {
   extern __shared__ uint4 smem_raw[];
@@ -48,7 +50,10 @@ __global__ void __launch_bounds__(512) k_prune(IndexView ix, RoundArgs ra, Prune
                           lay.ccap);
   Pm.sel = (uint4*)(base + lay.ws + prune_sel_offset(lay.ccap));
   const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
-  for (uint64_t b = gw; b < ra.B; b += (uint64_t)gridDim.x * wpc) {
+  uint64_t cur = gw;
+  const uint64_t step = (uint64_t)gridDim.x * wpc;
+  for (uint64_t b = warp_next_item(ra.qprune, cur, step); b < ra.B;
+       b = warp_next_item(ra.qprune, cur, step)) {
     const uint32_t p = (uint32_t)(ra.floor + b);
     load_vec(qv, ix.points + (uint64_t)p * ix.stride, qb);
     // the visited list, sorted by (dist, id) like the reference's
@@ -76,7 +81,7 @@ __global__ void __launch_bounds__(512) k_prune(IndexView ix, RoundArgs ra, Prune
     }
     __syncwarp();
     warp_std_sort(Pm, m);
-    warp_greedy_select_fast<DT, MT>(ix.points, ix.stride, ix.d, p, Pm, m, ra.alpha, ix.R,
+    warp_greedy_select_fast<DT, MT, true, TC>(ix.points, ix.stride, ix.d, p, Pm, m, ra.alpha, ix.R,
                                     ra.new_out + b * ix.Rp, ix.Rp, Pm.sel);
   }
 }
@@ -143,22 +148,39 @@ __global__ void __launch_bounds__(32) k_sort_rows(IndexView ix) {
   }
 }
 
-LaunchPlan plan_prune(const IndexView& ix, const PruneLayout& lay) {
+LaunchPlan plan_prune(const IndexView& ix, const PruneLayout& lay, bool tensor) {
   LaunchPlan p{1, 1};
-#define CALL(DT, MT) p = plan_warp_kernel(k_prune<DT, MT>, lay.total);
+#define CALL(DT, MT)                                                                 \
+  p = tensor ? plan_warp_kernel(k_prune<DT, MT, true>, lay.total)                    \
+             : plan_warp_kernel(k_prune<DT, MT, false>, lay.total);
   DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
 #undef CALL
   return p;
 }
 
-void launch_prune_round(const IndexView& ix, const RoundArgs& ra, const PruneLayout& lay,
-                        uint32_t vcap, const LaunchPlan& plan, int grid, cudaStream_t st) {
-  const size_t sm = (size_t)lay.total * plan.warps_per_cta;
+std::vector<LaunchPlan> prune_plan_candidates(const IndexView& ix, const PruneLayout& lay,
+                                              bool tensor) {
+  std::vector<LaunchPlan> v;
 #define CALL(DT, MT)                                                                 \
-  set_smem(k_prune<DT, MT>, sm);                                                     \
-  k_prune<DT, MT><<<grid, plan.warps_per_cta * 32, sm, st>>>(ix, ra, lay, vcap);
+  v = tensor ? warp_kernel_candidates(k_prune<DT, MT, true>, lay.total)              \
+             : warp_kernel_candidates(k_prune<DT, MT, false>, lay.total);
   DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
 #undef CALL
+  return v;
+}
+
+void launch_prune_round(const IndexView& ix, const RoundArgs& ra, const PruneLayout& lay,
+                        uint32_t vcap, const LaunchPlan& plan, int grid, bool tensor,
+                        cudaStream_t st) {
+  const size_t sm = (size_t)lay.total * plan.warps_per_cta;
+#define CALL2(DT, MT, TC)                                                            \
+  set_smem(k_prune<DT, MT, TC>, sm);                                                 \
+  k_prune<DT, MT, TC><<<grid, plan.warps_per_cta * 32, sm, st>>>(ix, ra, lay, vcap);
+#define CALL(DT, MT)                                                                 \
+  if (tensor) { CALL2(DT, MT, true); } else { CALL2(DT, MT, false); }
+  DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
+#undef CALL
+#undef CALL2
 }
 
 void launch_prune_tasks(const IndexView& ix, const PruneArgs& pa, cudaStream_t st) {

@@ -32,11 +32,11 @@ __global__ void k_apply_rows(uint32_t* graph, const uint32_t* new_out, uint64_t 
 struct RevLayout {
   uint32_t tv, cid, ckey, ws, total;
 };
-__host__ __device__ inline RevLayout rev_layout(uint32_t d, int dtype, uint32_t Rp) {
+__host__ __device__ inline RevLayout rev_layout(uint32_t d, int dtype, uint32_t Rp, bool tensor) {
   RevLayout r;
   uint32_t off = 0;
   uint32_t esz = dtype == DD_F32 ? 4 : 1;
-  const uint32_t sel_bytes = greedy_sel_bytes(d, dtype, Rp);
+  const uint32_t sel_bytes = greedy_sel_bytes(d, dtype, Rp, tensor);
   r.tv = off; off += r16((uint64_t)d * esz);
   r.cid = off; off += r16(4ull * kRevCandCap);
   r.ckey = off; off += r16(4ull * kRevCandCap);
@@ -54,7 +54,7 @@ __device__ __forceinline__ void segment_of(const ReverseScratch& rs, uint32_t k,
 
 // Append the sources of segment [start, end) (already in batch order), or
 // prune when the row would exceed R (one warp; s + deg <= kRevCandCap).
-template <int DT, int MT>
+template <int DT, int MT, bool TC>
 __device__ void reverse_one(const IndexView& ix, const RoundArgs& ra, const ReverseScratch& rs,
                             uint32_t t, uint32_t start, uint32_t s, uint32_t deg, uint8_t* tv,
                             PruneSmem Pm) {
@@ -83,7 +83,7 @@ __device__ void reverse_one(const IndexView& ix, const RoundArgs& ra, const Reve
   const uint32_t m = s + deg;
   warp_std_sort(Pm, m);
   // the candidate rows were just read for their distances to t: no prefetch
-  warp_greedy_select_fast<DT, MT, false>(ix.points, ix.stride, ix.d, t, Pm, m, ra.alpha, ix.R, row,
+  warp_greedy_select_fast<DT, MT, false, TC>(ix.points, ix.stride, ix.d, t, Pm, m, ra.alpha, ix.R, row,
                                          ix.Rp, Pm.sel);
   if (lane == 0) {
     atomicAdd(&rs.counters[2], 1u);
@@ -91,10 +91,10 @@ __device__ void reverse_one(const IndexView& ix, const RoundArgs& ra, const Reve
   }
 }
 
-template <int DT, int MT>
+template <int DT, int MT, bool TC>
 __global__ void __launch_bounds__(kRevWarps * 32, 8) k_reverse(IndexView ix, RoundArgs ra, ReverseScratch rs) {
   extern __shared__ uint4 smem_raw[];
-  const RevLayout L = rev_layout(ix.d, DT, ix.Rp);
+  const RevLayout L = rev_layout(ix.d, DT, ix.Rp, TC);
   const uint32_t wic = threadIdx.x >> 5, lane = lane_id();
   uint8_t* base = (uint8_t*)smem_raw + (size_t)wic * L.total;
   PruneSmem Pm = prune_ws((uint32_t*)(base + L.cid), (float*)(base + L.ckey), base + L.ws,
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(kRevWarps * 32, 8) k_reverse(IndexView ix, Rou
       }
       continue;  // handled by k_reverse_big
     }
-    reverse_one<DT, MT>(ix, ra, rs, t, start, s, deg, base + L.tv, Pm);
+    reverse_one<DT, MT, TC>(ix, ra, rs, t, start, s, deg, base + L.tv, Pm);
   }
 }
 
@@ -136,7 +136,7 @@ constexpr int kBigStackInts = 3 * 72;
 constexpr uint32_t kBigSelBytes = (kMaxRp + kMmaChunk) * 128u + (kMaxRp + kMmaChunk) * 4u +
                                   kMmaChunk * 4u;
 
-template <int DT, int MT>
+template <int DT, int MT, bool TC>
 __global__ void __launch_bounds__(kBigThreads) k_reverse_big(IndexView ix, RoundArgs ra, ReverseScratch rs) {
   __shared__ __align__(16) uint8_t tv[1024];
   __shared__ uint32_t sh[32];
@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(kBigThreads) k_reverse_big(IndexView ix, Round
         ddsort::insertion_sort_range(A, (int)q, ddsort::leaf_end(bits, (int)q, (int)m));
     __syncthreads();
     // ---- greedy selection (the row of t is rewritten; its old entries are in cid)
-    if (DT != DD_F32 && greedy_uses_mma(ix.d, DT)) {
+    if (TC && DT != DD_F32 && greedy_uses_mma(ix.d, DT)) {
       // chunked greedy on one warp: every candidate row is read once, and the
       // walk stops at the R-th selection (hub lists are far longer than that)
       if (wid == 0) {
@@ -319,17 +319,20 @@ void launch_apply_rows(const IndexView& ix, const RoundArgs& ra, cudaStream_t st
 }
 
 void launch_reverse(const IndexView& ix, const RoundArgs& ra, const ReverseScratch& rs,
-                    cudaStream_t st, int sm_count) {
+                    bool tensor, cudaStream_t st, int sm_count) {
   if (!ra.B) return;
-  RevLayout L = rev_layout(ix.d, ix.dtype, ix.Rp);
+  RevLayout L = rev_layout(ix.d, ix.dtype, ix.Rp, tensor);
   size_t sm = (size_t)L.total * kRevWarps;
+#define CALL2(DT, MT, TC)                                                             \
+  set_smem(k_reverse<DT, MT, TC>, sm);                                                \
+  k_reverse<DT, MT, TC><<<sm_count * occupancy(k_reverse<DT, MT, TC>, kRevWarps * 32, sm), \
+                          kRevWarps * 32, sm, st>>>(ix, ra, rs);                      \
+  k_reverse_big<DT, MT, TC><<<kBigSlots, kBigThreads, 0, st>>>(ix, ra, rs);
 #define CALL(DT, MT)                                                                  \
-  set_smem(k_reverse<DT, MT>, sm);                                                    \
-  k_reverse<DT, MT><<<sm_count * occupancy(k_reverse<DT, MT>, kRevWarps * 32, sm),     \
-                      kRevWarps * 32, sm, st>>>(ix, ra, rs);                          \
-  k_reverse_big<DT, MT><<<kBigSlots, kBigThreads, 0, st>>>(ix, ra, rs);
+  if (tensor) { CALL2(DT, MT, true); } else { CALL2(DT, MT, false); }
   DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
 #undef CALL
+#undef CALL2
 }
 
 }  // namespace ddk

@@ -110,7 +110,10 @@ __global__ void __launch_bounds__(512) k_search(IndexView ix, RoundArgs ra, Warp
   P.degree_limit = ix.R; P.hbits = lay.hbits; P.vcap = lay.vcap; P.query_mode = 0;
   P.keep_visited = 1; P.err = ix.err;
   const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
-  for (uint64_t b = gw; b < ra.B; b += (uint64_t)gridDim.x * wpc) {
+  uint64_t cur = gw;
+  const uint64_t step = (uint64_t)gridDim.x * wpc;
+  for (uint64_t b = warp_next_item(ra.qsearch, cur, step); b < ra.B;
+       b = warp_next_item(ra.qsearch, cur, step)) {
     const uint32_t p = (uint32_t)(ra.floor + b);
     const SearchSmem S = carve_build(base, lay, ra.vis_all + b * 2ull * lay.vcap);
     load_vec(S.qv, ix.points + (uint64_t)p * ix.stride, qb);
@@ -132,12 +135,17 @@ __global__ void __launch_bounds__(512) k_query(IndexView ix, QueryArgs qa, WarpL
   const uint64_t gw = (uint64_t)blockIdx.x * wpc + wic;
   const SearchSmem S = carve_query((uint8_t*)smem_raw + (size_t)wic * lay.total, lay);
   const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
-  for (uint64_t q = gw; q < qa.nq; q += (uint64_t)gridDim.x * wpc) {
+  const uint64_t nitems = qa.cls_items ? (uint64_t)*qa.cls_count : qa.nq;
+  uint64_t cur = gw;
+  const uint64_t step = (uint64_t)gridDim.x * wpc;
+  for (uint64_t it = warp_next_item(qa.cls_queue, cur, step); it < nitems;
+       it = warp_next_item(qa.cls_queue, cur, step)) {
+    const uint64_t q = qa.cls_items ? qa.cls_items[it] : it;
     SearchParams P;
     uint32_t Lq = qa.Ls[q];
-    if (Lq == 0 || Lq > qa.Lmax || Lq < qa.k) {
+    if (Lq == 0 || Lq > qa.Lvalid || Lq < qa.k) {
       if (lane == 0) dd_set_error(ix.err, DD_ECAND_CAP);
-      Lq = qa.Lmax;
+      Lq = qa.Lvalid;
     }
     P.points = ix.points; P.stride = ix.stride; P.graph = ix.graph; P.Rp = ix.Rp; P.n = ix.n;
     P.d = ix.d; P.start = qa.start; P.L = Lq; P.k = qa.k; P.cut = qa.cut; P.limit = qa.limit;
@@ -157,6 +165,23 @@ __global__ void __launch_bounds__(512) k_query(IndexView ix, QueryArgs qa, WarpL
     }
     __syncwarp();
   }
+}
+
+__global__ void k_bin_queries(const uint32_t* Ls, uint64_t nq, uint32_t k, uint32_t Lvalid,
+                              uint32_t* items, uint32_t* counts) {
+  for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq;
+       q += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t L = Ls[q];
+    if (L == 0 || L > Lvalid || L < k) L = Lvalid;
+    const int c = query_class(L);
+    items[(uint64_t)c * nq + atomicAdd(&counts[c], 1u)] = (uint32_t)q;
+  }
+}
+
+void launch_bin_queries(const uint32_t* Ls, uint64_t nq, uint32_t k, uint32_t Lvalid,
+                        uint32_t* items, uint32_t* counts, cudaStream_t st) {
+  const int grid = (int)std::min<uint64_t>((nq + 255) / 256, 1024);
+  k_bin_queries<<<grid, 256, 0, st>>>(Ls, nq, k, Lvalid, items, counts);
 }
 
 template <int DT, int MT>
@@ -211,6 +236,17 @@ LaunchPlan plan_search(const IndexView& ix, const WarpLayout& lay, uint32_t L) {
 #undef CALL
 #undef CALL4
   return p;
+}
+
+std::vector<LaunchPlan> search_plan_candidates(const IndexView& ix, const WarpLayout& lay,
+                                               uint32_t L) {
+  std::vector<LaunchPlan> v;
+#define CALL4(DT, MT, F, C) v = warp_kernel_candidates(k_search<DT, MT, F, C>, lay.total);
+#define CALL(DT, MT) DD_DISPATCH_FC(L, ix.Rp, DT, MT, CALL4)
+  DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
+#undef CALL
+#undef CALL4
+  return v;
 }
 
 void launch_search(const IndexView& ix, const RoundArgs& ra, const WarpLayout& lay,

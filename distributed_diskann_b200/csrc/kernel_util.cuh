@@ -3,6 +3,7 @@
 #pragma once
 #include <algorithm>
 #include <cstdint>
+#include <vector>
 
 #include "dd_common.cuh"
 #include "kernels.cuh"
@@ -29,6 +30,20 @@ __device__ __forceinline__ uint32_t row_degree(const uint32_t* row, uint32_t Rp)
     deg += __popc(__ballot_sync(0xffffffffu, v));
   }
   return deg;
+}
+
+// The next work item of a warp: from the device queue `q` (one atomic by
+// lane 0, broadcast) when the launch is persistent, else the static
+// grid-stride sequence cur, cur + step, ...  `q` is uniform over the launch.
+__device__ __forceinline__ uint64_t warp_next_item(uint32_t* q, uint64_t& cur, uint64_t step) {
+  if (q) {
+    uint32_t v = 0;
+    if (lane_id() == 0) v = atomicAdd(q, 1u);
+    return __shfl_sync(0xffffffffu, v, 0);
+  }
+  const uint64_t r = cur;
+  cur += step;
+  return r;
 }
 
 #define DD_DISPATCH_DM(dtype, metric, CALL)                                          \
@@ -78,6 +93,21 @@ static LaunchPlan plan_warp_kernel(K kernel, uint32_t bytes_per_warp) {
   }
   if (best.blocks_per_sm == 0) best.blocks_per_sm = 1;
   return best;
+}
+
+// The CTA shapes the autotuner times for a per-warp kernel: 2, 4, 8 and 16
+// warps per CTA, each with the CTAs per SM the occupancy API allows.
+template <typename K>
+static std::vector<LaunchPlan> warp_kernel_candidates(K kernel, uint32_t bytes_per_warp) {
+  std::vector<LaunchPlan> v;
+  static const int cand[] = {2, 4, 8, 16};
+  for (int wpc : cand) {
+    const size_t sm = (size_t)bytes_per_warp * wpc;
+    if (sm > 227 * 1024) break;
+    const int b = occupancy(kernel, wpc * 32, sm);
+    if (b >= 1) v.push_back(LaunchPlan{wpc, b});
+  }
+  return v;
 }
 
 }  // namespace ddk

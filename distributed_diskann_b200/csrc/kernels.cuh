@@ -1,6 +1,7 @@
 // Host-visible launch interface of the device kernels (kernels.cu).
 #pragma once
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 namespace ddk {
@@ -46,7 +47,8 @@ struct IndexView {
 // k_query only needs the evicted list)
 WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, uint32_t vcap,
                               bool build, bool h24, bool keep_vis = true);
-PruneLayout make_prune_layout(uint32_t d, int dtype, uint32_t Rp, uint32_t ccap);
+// tensor: the fast form's tensor-core greedy (integer data); false: the plain form
+PruneLayout make_prune_layout(uint32_t d, int dtype, uint32_t Rp, uint32_t ccap, bool tensor);
 
 
 struct RoundArgs {
@@ -59,6 +61,11 @@ struct RoundArgs {
   uint32_t* stat_vis;    // B visited-list lengths (k_search writes, k_prune reads)
   uint32_t* stat_cmps;   // B (may be null)
   uint32_t* vis_all;     // per batch point: vcap visited ids, then vcap distances
+  // device work queues (zeroed before the round): with a queue the launch is
+  // persistent and each warp takes its next batch point from the counter;
+  // null = static grid-stride assignment
+  uint32_t* qsearch;
+  uint32_t* qprune;
 };
 
 // The round's reverse edges grouped by target (see semisort.cuh): segment k
@@ -88,15 +95,21 @@ constexpr uint32_t kBigThreads = 512;   // threads per CTA of the big-target pat
 constexpr uint32_t kBigSlots = 148;     // CTAs (and workspace slices) of the big-target path
 
 LaunchPlan plan_search(const IndexView& ix, const WarpLayout& lay, uint32_t L);
+// the CTA shapes an autotuner may time (see warp_kernel_candidates)
+std::vector<LaunchPlan> search_plan_candidates(const IndexView& ix, const WarpLayout& lay,
+                                               uint32_t L);
+std::vector<LaunchPlan> prune_plan_candidates(const IndexView& ix, const PruneLayout& lay,
+                                              bool tensor);
 void launch_search(const IndexView& ix, const RoundArgs& ra, const WarpLayout& lay,
                    const LaunchPlan& plan, int grid, cudaStream_t st);
-LaunchPlan plan_prune(const IndexView& ix, const PruneLayout& lay);
+LaunchPlan plan_prune(const IndexView& ix, const PruneLayout& lay, bool tensor);
 void launch_prune_round(const IndexView& ix, const RoundArgs& ra, const PruneLayout& lay,
-                        uint32_t vcap, const LaunchPlan& plan, int grid, cudaStream_t st);
+                        uint32_t vcap, const LaunchPlan& plan, int grid, bool tensor,
+                        cudaStream_t st);
 void launch_apply_rows(const IndexView& ix, const RoundArgs& ra, cudaStream_t st);
 // append-or-prune per target over the segments the semisort produced
 void launch_reverse(const IndexView& ix, const RoundArgs& ra, const ReverseScratch& rs,
-                    cudaStream_t st, int sm_count);
+                    bool tensor, cudaStream_t st, int sm_count);
 
 struct QueryArgs {
   const uint8_t* queries;  // device rows, stride qstride (zero padded to 16 bytes)
@@ -114,7 +127,28 @@ struct QueryArgs {
   float* dists;            // nq x k
   uint32_t* visited;       // nq (may be null)
   uint32_t* cmps;          // nq (may be null)
+  // beam-width class of the launch (fast form): the launch serves the
+  // queries listed in cls_items[0, *cls_count), taken from the work queue
+  // cls_queue; null = every query, grid-stride
+  const uint32_t* cls_items;
+  const uint32_t* cls_count;
+  uint32_t* cls_queue;
+  uint32_t Lvalid;         // largest valid beam width (the caller's Lmax; Lmax is the class's)
 };
+
+// Beam-width classes of the bucketed query launch: class c serves beam widths
+// in (16 << (c-1), 16 << c]; its launch is laid out for 16 << c.
+constexpr int kQueryClasses = 6;
+__host__ __device__ inline int query_class(uint32_t L) {
+  int c = 0;
+  while (c + 1 < kQueryClasses && L > (16u << c)) c++;
+  return c;
+}
+// Lists the queries of each class: items[c * nq + i], counts[c] (zeroed before).
+// A query whose beam width is invalid (0, below k or above Lvalid) goes to the
+// class of Lvalid, whose launch reports it.
+void launch_bin_queries(const uint32_t* Ls, uint64_t nq, uint32_t k, uint32_t Lvalid,
+                        uint32_t* items, uint32_t* counts, cudaStream_t st);
 LaunchPlan plan_query(const IndexView& ix, const WarpLayout& lay, uint32_t Lmax);
 void launch_query(const IndexView& ix, const QueryArgs& qa, const WarpLayout& lay,
                   int warps_per_cta, int grid, cudaStream_t st);

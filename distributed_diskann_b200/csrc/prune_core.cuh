@@ -506,9 +506,11 @@ __host__ __device__ inline uint32_t mma_sel_bytes(uint32_t Rp) {
 __host__ __device__ inline bool greedy_uses_mma(uint32_t d, int dtype) {
   return dtype != DD_F32 && d <= 128;
 }
-// bytes the fast greedy forms need in the prune workspace (0: generic form)
-__host__ __device__ inline uint32_t greedy_sel_bytes(uint32_t d, int dtype, uint32_t Rp) {
-  if (greedy_uses_mma(d, dtype)) return mma_sel_bytes(Rp);
+// bytes the fast greedy forms need in the prune workspace (0: generic form);
+// tensor = false leaves the tensor-core form out (the plain form)
+__host__ __device__ inline uint32_t greedy_sel_bytes(uint32_t d, int dtype, uint32_t Rp,
+                                                     bool tensor = true) {
+  if (tensor && greedy_uses_mma(d, dtype)) return mma_sel_bytes(Rp);
   const uint32_t nv = row_words16(d, dtype);
   return nv <= reg_row_max_words(dtype) ? Rp * nv * 16u : 0u;
 }
@@ -751,20 +753,21 @@ __device__ uint32_t warp_greedy_select_mma(const uint8_t* points, uint64_t strid
 }
 
 // The fastest exact greedy form for the data type; `sel` holds
-// greedy_sel_bytes(d, DT, Rp) bytes (unused by the generic form).  PREFETCH:
+// greedy_sel_bytes(d, DT, Rp, TENSOR) bytes (unused by the generic form).
+// TENSOR = false is the plain form: every occlusion distance on the CUDA
+// cores (register rows where they fit, else the per-lane form).  PREFETCH:
 // see warp_greedy_select_mma.
-template <int DT, int MT, bool PREFETCH = true>
+template <int DT, int MT, bool PREFETCH = true, bool TENSOR = true>
 __device__ __forceinline__ uint32_t warp_greedy_select_fast(const uint8_t* points, uint64_t stride,
                                                             uint32_t d, uint32_t p,
                                                             const PruneSmem& S, uint32_t m,
                                                             double alpha, uint32_t R,
                                                             uint32_t* out_row, uint32_t Rp,
                                                             uint4* sel) {
-  if (DT != DD_F32) {
-    if (greedy_uses_mma(d, DT))
-      return warp_greedy_select_mma<DT, MT, PREFETCH>(points, stride, d, p, S, m, alpha, R,
-                                                      out_row, Rp, sel);
-  } else if (row_words16(d, DT) <= (uint32_t)RegRow<DT>::NVM) {
+  if (TENSOR && DT != DD_F32 && greedy_uses_mma(d, DT))
+    return warp_greedy_select_mma<DT, MT, PREFETCH>(points, stride, d, p, S, m, alpha, R,
+                                                    out_row, Rp, sel);
+  if (row_words16(d, DT) <= (uint32_t)RegRow<DT>::NVM) {
     return warp_greedy_select_reg<DT, MT>(points, stride, d, p, S, m, alpha, R, out_row, Rp, sel);
   }
   return warp_greedy_select<DT, MT>(points, stride, d, p, S, m, alpha, R, out_row, Rp);

@@ -88,6 +88,13 @@ class GpuIndex:
     def set_stream(self, stream_ptr: int):
         self._ck(self.lib.dd_set_stream(self.h, C.c_void_p(stream_ptr)))
 
+    def set_search_mode(self, mode: str):
+        self._ck(self.lib.dd_set_search_mode(self.h, L.MODES[mode]))
+
+    def check_errors(self):
+        """Raises if a kernel of an asynchronous call raised the device error word."""
+        self._ck(self.lib.dd_check_errors(self.h))
+
     def graph(self) -> np.ndarray:
         g = np.zeros((self.n, self.R + 1), np.uint32)
         self._ck(self.lib.dd_download_graph(self.h, _ptr(g)))
@@ -106,10 +113,12 @@ class GpuIndex:
 
     # ---------------------------------------------------------------- build
     def build(self, L_, alpha, max_fraction=1.0, max_build=0, start_point=0, two_pass=False,
-              knn_mode=False, collect_stats=True, vcap=0) -> dict:
+              knn_mode=False, collect_stats=True, vcap=0, mode="fast") -> dict:
+        """Batched build; mode "fast" (tensor-core tiles, persistent kernels,
+        graph-captured rounds) or "plain" (CUDA-core exact form): same graph."""
         p = L.BuildParamsC(int(L_), float(alpha), float(max_fraction), int(max_build),
                            int(start_point), int(two_pass), int(knn_mode), int(collect_stats),
-                           int(vcap))
+                           int(vcap), L.MODES[mode])
         st = L.StatsC()
         self._ck(self.lib.dd_build(self.h, C.byref(p), C.byref(st)))
         return st.as_dict()

@@ -37,6 +37,19 @@ extern "C" {
 #define DD_ERR_UNSUPPORTED 5  /* parameter outside the supported range */
 #define DD_ERR_IO 6           /* file could not be read or written */
 
+/* computation forms (dd_build_params.mode, dd_set_search_mode).  Both give
+ * the same graph and the same search results, bit for bit:
+ *   DD_MODE_FAST  : tensor-core distance tiles where they apply (INT8 Gram
+ *                   tiles of robustPrune for integer data), persistent kernels
+ *                   fed by a device work queue, each build captured as one CUDA
+ *                   graph, autotuned CTA shapes, queries bucketed by beam width;
+ *   DD_MODE_PLAIN : every distance on the CUDA cores, grid-stride kernels
+ *                   launched round by round, one query launch sized for the
+ *                   largest beam width (the exact form the fast one is checked
+ *                   and timed against). */
+#define DD_MODE_FAST 0
+#define DD_MODE_PLAIN 1
+
 /* element types (the reference's dtype dispatch, src/diskann.cpp:118-120) */
 #define DD_DTYPE_F32 0
 #define DD_DTYPE_I8 1
@@ -60,6 +73,7 @@ typedef struct dd_build_params {
   int32_t knn_mode;      /* 1: knn_index::build_index (max_fraction 1, sorted rows) */
   int32_t collect_stats; /* 1: fill visited / distance-count statistics */
   uint32_t vcap;         /* visited-list capacity per search, 0 = 4 * L */
+  int32_t mode;          /* DD_MODE_FAST (0) or DD_MODE_PLAIN */
 } dd_build_params;
 
 typedef struct dd_stats {
@@ -75,6 +89,11 @@ typedef struct dd_stats {
   double reverse_ms;       /* device time of the reverse-edge kernels */
   double search_ms;        /* device time of the insert beam searches alone (part of
                               search_prune_ms) */
+  uint32_t search_warps_per_cta; /* CTA shape of the insert searches (autotuned: fast form) */
+  uint32_t prune_warps_per_cta;  /* CTA shape of the insert prunes */
+  int32_t search_queue;    /* 1: persistent searches fed by a device work queue */
+  int32_t prune_queue;     /* 1: persistent prunes fed by a device work queue */
+  int32_t graph_replay;    /* 1: the build ran as one replayed CUDA graph */
 } dd_stats;
 
 /* ------------------------------------------------------------------ handle */
@@ -86,6 +105,12 @@ int dd_destroy(dd_index* h);
 const char* dd_last_error(const dd_index* h);
 /* all work of the handle is issued on this CUDA stream (cudaStream_t); 0 = default */
 int dd_set_stream(dd_index* h, void* stream);
+/* form of dd_search / dd_search_device (DD_MODE_FAST by default) */
+int dd_set_search_mode(dd_index* h, int mode);
+/* waits for the handle's stream and reports the device error word that the
+ * asynchronous entry points (dd_search_device) leave: DD_ERR_DEVICE with the
+ * message when a kernel raised it since the last check, else DD_OK */
+int dd_check_errors(dd_index* h);
 
 /* ------------------------------------------------------------------ data */
 /* PointRange: copies n rows of d elements; row_stride_bytes between rows */

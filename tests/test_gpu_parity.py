@@ -28,14 +28,17 @@ def gpu_build(base, R, L, alpha, metric="l2", **kw):
     return gi, canon(gi.graph()), st
 
 
+@pytest.mark.parametrize("mode", ["fast", "plain"])
 @pytest.mark.parametrize("name", list(BUILD_CASES))
-def test_build_and_search_bit_exact_vs_reference(golden, name):
+def test_build_and_search_bit_exact_vs_reference(golden, name, mode):
+    """Both computation forms (DD_MODE_FAST, DD_MODE_PLAIN) against the reference."""
     g, arrays = golden
     rec = g["cases"][name]
     R, L, alpha, metric, xita, mx, st, knn, tp, Ls = BUILD_CASES[name]
     base, queries = case_inputs(name)
     gi, graph, stats = gpu_build(base, R, L, alpha, metric=metric, max_fraction=xita, max_build=mx,
-                                 start_point=st, knn_mode=knn, two_pass=tp)
+                                 start_point=st, knn_mode=knn, two_pass=tp, mode=mode)
+    gi.set_search_mode(mode)
     if f"{name}__graph" in arrays:
         np.testing.assert_array_equal(graph, arrays[f"{name}__graph"])
     assert sha(graph) == rec["graph_sha256"], f"{name}: graph differs from the reference build"
@@ -114,12 +117,16 @@ def test_groundtruth_vs_oracle(oracle_mod, dtype, metric):
     gi.close()
 
 
-def test_mixed_beam_widths_in_one_launch(golden):
+@pytest.mark.parametrize("mode", ["fast", "plain"])
+def test_mixed_beam_widths_in_one_call(golden, mode):
+    """Mixed beam widths in one call: one launch sized for the largest width
+    (plain form) or one persistent launch per beam-width class (fast form)."""
     g, _ = golden
     base, queries = case_inputs("i8_small")
     gi = GpuIndex(base.dtype, "l2", base.shape[0], base.shape[1], 64)
     gi.upload_points(base)
     gi.build(128, 1.2)
+    gi.set_search_mode(mode)
     Ls = np.array([10, 20, 50, 100, 200], np.uint32)[np.arange(len(queries)) % 5]
     ids_mixed, _, vis_m, cm_m = gi.search(queries, 10, Ls)
     for L in (10, 20, 50, 100, 200):
@@ -175,14 +182,40 @@ def test_mid_size_int8_build_bit_exact_vs_oracle(oracle_mod):
     gi.close()
 
 
-def test_mid_size_uint8_build_bit_exact_vs_oracle(oracle_mod):
+@pytest.mark.parametrize("mode", ["fast", "plain"])
+def test_mid_size_uint8_build_bit_exact_vs_oracle(oracle_mod, mode):
     """120k x 128 uint8 with the skewed non-negative values of the BIGANN-shaped
-    workload (u8 x u8 tensor-core tiles), hub targets included."""
+    workload, hub targets included: u8 x u8 tensor-core tiles in the fast form,
+    CUDA-core occlusion distances in the plain form."""
     base = D.gen_skewed_u8(120_000, 128, 1200, 6)
-    gi, graph, st = gpu_build(base, 64, 128, 1.2)
+    gi, graph, st = gpu_build(base, 64, 128, 1.2, mode=mode)
     og, ost = oracle_mod.build(base, 64, 128, 1.2)
     np.testing.assert_array_equal(graph, canon(og))
     assert st["big_groups"] > 0 and st["reverse_prunes"] > 0
+    if mode == "fast":
+        # the first fast build of this shape calibrated the CTA shapes; builds
+        # without statistics then run as one captured CUDA graph, replayed
+        for _ in range(2):
+            st2 = gi.build(128, 1.2, collect_stats=False, mode="fast")
+            assert st2["graph_replay"] == 1
+            np.testing.assert_array_equal(canon(gi.graph()), graph)
+    gi.close()
+
+
+def test_graph_replayed_fast_build_matches_reference(golden):
+    """Fast builds without statistics are captured once as a CUDA graph and
+    replayed: the replays give the reference's graph, as the stream path does."""
+    g, _ = golden
+    base, _ = case_inputs("i8_small")
+    gi = GpuIndex(base.dtype, "l2", base.shape[0], base.shape[1], 64)
+    gi.upload_points(base)
+    for _ in range(3):
+        st = gi.build(128, 1.2, collect_stats=False, mode="fast")
+        assert st["graph_replay"] == 1
+        assert sha(canon(gi.graph())) == g["cases"]["i8_small"]["graph_sha256"]
+    st = gi.build(128, 1.2, collect_stats=True, mode="fast")
+    assert st["graph_replay"] == 0
+    assert sha(canon(gi.graph())) == g["cases"]["i8_small"]["graph_sha256"]
     gi.close()
 
 
