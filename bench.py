@@ -50,6 +50,12 @@ def parse():
     ap.add_argument("--no-queries", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline work budget")
+    ap.add_argument("--no-cpu-queries", action="store_true",
+                    help="skip the reference's query QPS in the CPU baseline")
+    ap.add_argument("--cpu-nq", type=int, default=2000,
+                    help="queries of the reference's timed query sweep")
+    ap.add_argument("--plain-steps", type=int, default=3,
+                    help="timed builds of the plain exact form (capped by --steps)")
     return ap.parse_args()
 
 
@@ -176,6 +182,38 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def reference_cpu_queries(base, graph, queries, gt_i, gt_d, w, nq):
+    """The reference's searchAll timed like checkRecall (untimed pass, then a
+    timed one) at each beam width of the sweep, on the built graph (identical
+    to the reference's own build) with the first `nq` queries, all host
+    threads; recall@10 with ties against the brute-force ground truth (the
+    GPU's exact one, which the tests pin to the oracle's)."""
+    from oracle import oracle as O
+
+    cores = os.cpu_count() or 1
+    nq = min(nq, queries.shape[0])
+    q = np.ascontiguousarray(queries[:nq])
+    res = O.ref_qps(base, graph, q, 10, list(w.sweep_L), cut=1.35, metric=w.metric,
+                    threads=cores)
+    gt_i, gt_d = gt_i[:nq], gt_d[:nq]
+    sweep = []
+    for L in w.sweep_L:
+        ids, secs = res[L]
+        sweep.append({"L": L, "qps": nq / secs,
+                      "recall10": D_recall(ids, gt_i, gt_d)})
+    ok = [s for s in sweep if s["recall10"] >= 0.95]
+    return {"qps_at_recall10_0.95": max(s["qps"] for s in ok) if ok else None,
+            "sweep": sweep, "unit": "queries/s", "cores": cores, "kind": "reference",
+            "sample": f"first {nq} of the {queries.shape[0]} queries on the full built graph "
+                      f"(reference searchAll, PARLAY_NUM_THREADS={cores})"}
+
+
+def D_recall(ids, gt_i, gt_d):
+    from distributed_diskann_b200 import datasets as D
+
+    return D.recall_with_ties(ids, gt_i, gt_d, 10)
+
+
 # ---------------------------------------------------------------------- our arm
 def main():
     args = parse()
@@ -223,9 +261,10 @@ def main():
     def max_over_ranks(x):
         return MR.max_over_ranks(x, dev, world > 1)
 
-    # ---- warm-up
+    # ---- warm-up (the first fast build calibrates the CTA shapes; the next one
+    # captures the build as a CUDA graph, which the timed builds replay)
     for _ in range(args.warmup):
-        gi.build(w.L, w.alpha, collect_stats=False)
+        gi.build(w.L, w.alpha, collect_stats=False, mode="fast")
     barrier()
 
     # ---- timed builds, inputs resident in HBM
@@ -236,7 +275,7 @@ def main():
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
-        gi.build(w.L, w.alpha, collect_stats=False)
+        gi.build(w.L, w.alpha, collect_stats=False, mode="fast")
         launches += gi.launches()
     ev1.record(stream)
     ev1.synchronize()
@@ -250,7 +289,7 @@ def main():
     ev0.record(stream)
     for _ in range(args.steps):
         gi.lib.dd_upload_points(gi.h, base_t.data_ptr(), base_t.stride(0) * base_t.element_size())
-        gi.build(w.L, w.alpha, collect_stats=False)
+        gi.build(w.L, w.alpha, collect_stats=False, mode="fast")
         gi.lib.dd_download_graph(gi.h, graph_host.data_ptr())
     ev1.record(stream)
     ev1.synchronize()
@@ -259,8 +298,24 @@ def main():
     h2d = base.nbytes
     d2h = n * (w.R + 1) * 4
 
+    # ---- the plain exact form (CUDA-core distances, grid-stride kernels launched
+    # round by round): same graph; timed on min(steps, plain_steps) builds
+    graph_fast = gi.graph()
+    ksp = max(1, min(args.steps, args.plain_steps))
+    gi.build(w.L, w.alpha, collect_stats=False, mode="plain")
+    barrier()
+    ev0.record(stream)
+    for _ in range(ksp):
+        gi.build(w.L, w.alpha, collect_stats=False, mode="plain")
+    ev1.record(stream)
+    ev1.synchronize()
+    t_plain = max_over_ranks(ev0.elapsed_time(ev1) / 1000.0)
+    plain_value = MR.whole_job_rate(world, n, ksp, t_plain)
+    plain_same = bool(np.array_equal(gi.graph(), graph_fast))
+    st_plain = gi.build(w.L, w.alpha, collect_stats=True, mode="plain")
+
     # ---- one instrumented build: statistics + per-kernel device times
-    st = gi.build(w.L, w.alpha, collect_stats=True)
+    st = gi.build(w.L, w.alpha, collect_stats=True, mode="fast")
     g = gi.graph()
     deg = g[:, 0]
     es = 4 if w.dtype == "f32" else 1
@@ -298,32 +353,35 @@ def main():
         qstride = qpad.stride(0) * qpad.element_size()
         ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
         dd = torch.empty((nq, k), dtype=torch.float32, device=dev)
-        sweep = []
-        for L in w.sweep_L:
-            Ls = torch.full((nq,), L, dtype=torch.int32, device=dev)
+        def timed_search(Ls, Lmax):
             for _ in range(2):  # first run warms up; the second is timed (checkRecall)
                 torch.cuda.synchronize(dev)  # rank 0 only: no collective here
                 ev0.record(stream)
-                gi.search_device(qpad.data_ptr(), nq, qstride, Ls.data_ptr(), L, k,
+                gi.search_device(qpad.data_ptr(), nq, qstride, Ls.data_ptr(), Lmax, k,
                                  ids.data_ptr(), dd.data_ptr())
                 ev1.record(stream)
                 ev1.synchronize()
-            t = ev0.elapsed_time(ev1) / 1000.0
-            rec = D.recall_with_ties(ids.cpu().numpy().astype(np.uint32), gt_i, gt_d, k)
-            sweep.append({"L": L, "qps": nq / t, "recall10": rec})
-        Ls = torch.tensor(np.array(w.sweep_L, np.int32)[np.arange(nq) % len(w.sweep_L)],
-                          device=dev)
-        torch.cuda.synchronize(dev)
-        ev0.record(stream)
-        gi.search_device(qpad.data_ptr(), nq, qstride, Ls.data_ptr(), max(w.sweep_L), k,
-                         ids.data_ptr(), dd.data_ptr())
-        ev1.record(stream)
-        ev1.synchronize()
-        mixed_qps = nq / (ev0.elapsed_time(ev1) / 1000.0)
-        ok = [s for s in sweep if s["recall10"] >= 0.95]
-        qres = {"sweep": sweep, "mixed_L_qps": mixed_qps,
-                "qps_at_recall10_0.95": max(s["qps"] for s in ok) if ok else None,
-                "nq": nq, "k": k, "cut": 1.35}
+            gi.check_errors()  # the device error word of the asynchronous search
+            return ev0.elapsed_time(ev1) / 1000.0
+
+        Lmix = torch.tensor(np.array(w.sweep_L, np.int32)[np.arange(nq) % len(w.sweep_L)],
+                            device=dev)
+        qres = {"nq": nq, "k": k, "cut": 1.35}
+        for form in ("fast", "plain"):
+            gi.set_search_mode(form)
+            sweep = []
+            for L in w.sweep_L:
+                Ls = torch.full((nq,), L, dtype=torch.int32, device=dev)
+                t = timed_search(Ls, L)
+                rec = D.recall_with_ties(ids.cpu().numpy().astype(np.uint32), gt_i, gt_d, k)
+                sweep.append({"L": L, "qps": nq / t, "recall10": rec})
+            t = timed_search(Lmix, max(w.sweep_L))
+            ok = [s for s in sweep if s["recall10"] >= 0.95]
+            qres[form] = {"sweep": sweep, "mixed_L_qps": nq / t,
+                          "qps_at_recall10_0.95": max(s["qps"] for s in ok) if ok else None}
+        gi.set_search_mode("fast")
+        qres["qps_at_recall10_0.95"] = qres["fast"]["qps_at_recall10_0.95"]
+        qres["mixed_L_qps"] = qres["fast"]["mixed_L_qps"]
 
     # ---- CPU baseline: the reference's own build on a sample, rank 0, N = 1
     cpu = None
@@ -337,6 +395,12 @@ def main():
         except Exception as e:  # reported, never fatal for the GPU numbers
             cpu = {"value": None, "unit": "points/s", "cores": os.cpu_count(),
                    "kind": "reference", "sample": f"unavailable: {e}"}
+        if qres is not None and not args.no_cpu_queries:
+            try:
+                cpu["queries"] = reference_cpu_queries(base, g, queries, gt_i, gt_d, w,
+                                                       args.cpu_nq)
+            except Exception as e:  # reported, never fatal for the GPU numbers
+                cpu["queries"] = {"unavailable": str(e)}
 
     if rank == 0:
         line = {
@@ -347,7 +411,9 @@ def main():
             "config": {"workload": f"{w.name}: {n}x{w.d} {w.dtype} {w.metric}, R={w.R}, "
                                    f"L={w.L}, alpha={w.alpha} (full batched build per step)",
                        "n": n, "d": w.d, "R": w.R, "L": w.L, "alpha": w.alpha,
-                       "form": "plain exact (bit-exact vs the reference build)",
+                       "form": "fast (INT8 tensor-core prune tiles, persistent work-queue "
+                               "kernels, CUDA-graph build replay, autotuned CTA shapes); graph "
+                               "bit-exact vs the reference build",
                        "l2_flush": "inputs larger than L2 (points + graph > 126 MB)",
                        "parallelism": f"{world} independent partitions" if world > 1 else "1 GPU"},
             "e2e": {"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": h2d,
@@ -360,6 +426,22 @@ def main():
                                                  "reverse_prunes", "prune_cands", "big_groups",
                                                  "build_ms", "search_prune_ms", "search_ms", "reverse_ms")},
             "graph": {"avg_degree": float(deg.mean()), "max_degree": int(deg.max())},
+            "plain": {"value": plain_value, "unit": "points/s", "steps": ksp,
+                      "ms_per_step": 1000.0 * t_plain / ksp,
+                      "same_graph_as_fast": plain_same,
+                      "build_stats": {k2: st_plain[k2] for k2 in ("build_ms", "search_ms",
+                                                                  "search_prune_ms", "reverse_ms")},
+                      "form": "plain exact (CUDA-core distances, grid-stride kernels launched "
+                              "round by round)"},
+            "fast_over_plain": {"build": value / plain_value,
+                                "qps_at_recall10_0.95": (
+                                    qres["fast"]["qps_at_recall10_0.95"]
+                                    / qres["plain"]["qps_at_recall10_0.95"]
+                                    if qres and qres["plain"]["qps_at_recall10_0.95"] else None),
+                                "mixed_L_qps": (qres["fast"]["mixed_L_qps"]
+                                                / qres["plain"]["mixed_L_qps"] if qres else None)},
+            "tuned": {k2: st[k2] for k2 in ("search_warps_per_cta", "prune_warps_per_cta",
+                                            "search_queue", "prune_queue")},
             "queries": qres,
             "setup_s": {"datagen": gen_s},
         }

@@ -342,7 +342,7 @@ std::vector<std::pair<std::vector<uint64_t>, TuneResult>> g_tune;
 
 std::vector<uint64_t> tune_key(const dd_index* h, const BuildPlan& bp, uint32_t L) {
   return {(uint64_t)h->dtype, (uint64_t)h->metric, h->d, h->Rp, L, bp.slay.vcap, bp.slay.h24,
-          (uint64_t)bp.fast, (uint64_t)h->device};
+          bp.slay.fastf, bp.slay.total, bp.play.total, (uint64_t)bp.fast, (uint64_t)h->device};
 }
 
 bool tune_lookup(const std::vector<uint64_t>& key, TuneResult* out) {
@@ -741,11 +741,14 @@ int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
   if (rc) return rc;
   uint32_t vcap = P->vcap ? P->vcap : 4 * P->L;
   BuildPlan bp;
-  bp.slay = make_search_layout(h->d, h->dtype, P->L, h->Rp, vcap, true, use_h24(h));
+  bp.fast = P->mode == DD_MODE_FAST;
+  // the fast form's seen filter needs ids below 2^24 and rows without repeats
+  // (single-pass builds); two-pass builds replay the reference's filter
+  const bool fastf = bp.fast && use_h24(h) && !P->two_pass;
+  bp.slay = make_search_layout(h->d, h->dtype, P->L, h->Rp, vcap, true, use_h24(h), true, fastf);
   if (bp.slay.total > 227 * 1024)
     return fail(h, DD_ERR_UNSUPPORTED, "per-warp shared memory %u B too large (L=%u)",
                 bp.slay.total, P->L);
-  bp.fast = P->mode == DD_MODE_FAST;
   bp.play = make_prune_layout(h->d, h->dtype, h->Rp, bp.slay.ccap, bp.fast);
   if (bp.play.total > 227 * 1024)
     return fail(h, DD_ERR_UNSUPPORTED, "prune shared memory %u B too large (visited capacity %u)",

@@ -24,7 +24,7 @@ namespace ddk {
 // With h24 the hash table stores 24-bit ids (3 bytes a slot instead of 4),
 // which is exact whenever every id is below 0xFFFFFF.
 WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, uint32_t vcap,
-                              bool build, bool h24, bool keep_vis) {
+                              bool build, bool h24, bool keep_vis, bool fastf) {
   WarpLayout w{};
   uint32_t esz = dtype == DD_F32 ? 4 : 1;
   uint32_t off = 0;
@@ -39,7 +39,9 @@ WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, ui
   w.ccap = vcap + Rp;
   w.hbits = hash_bits_for(L);
   w.h24 = h24 ? 1u : 0u;
-  const uint32_t hash_bytes = r16(hash_table_bytes(w.hbits, h24));
+  w.fastf = (build && fastf) ? 1u : 0u;
+  const uint32_t hash_bytes =
+      r16(w.fastf ? fast_table_bytes(w.hbits) : hash_table_bytes(w.hbits, h24));
   if (build) {
     w.vis_id = w.vis_d = 0;  // global
     w.ws = off;
@@ -97,8 +99,12 @@ __device__ __forceinline__ SearchSmem carve_query(uint8_t* base, const WarpLayou
 // k_search: one warp per batch point runs beam_search on the round-start graph
 // and leaves its visited list in the point's global slice
 // (include/index.h:274-278; src/bsp_index.hpp:259-268).
-template <int DT, int MT, int FPL, int CPL>
-__global__ void __launch_bounds__(512) k_search(IndexView ix, RoundArgs ra, WarpLayout lay) {
+// FASTF: the fast form's seen filter, with registers capped so that 22
+// searches (two 11-warp CTAs) fit an SM, the most its shared memory holds at
+// L = 128 with that filter's 8 KB table.
+template <int DT, int MT, int FPL, int CPL, bool FASTF>
+__global__ void __launch_bounds__(FASTF ? 352 : 512, FASTF ? 2 : 1)
+    k_search(IndexView ix, RoundArgs ra, WarpLayout lay) {
   extern __shared__ uint4 smem_raw[];
   const uint32_t wpc = blockDim.x >> 5;
   const uint32_t wic = threadIdx.x >> 5;
@@ -118,7 +124,7 @@ __global__ void __launch_bounds__(512) k_search(IndexView ix, RoundArgs ra, Warp
     const SearchSmem S = carve_build(base, lay, ra.vis_all + b * 2ull * lay.vcap);
     load_vec(S.qv, ix.points + (uint64_t)p * ix.stride, qb);
     __syncwarp();
-    const SearchOut o = warp_beam_search<DT, MT, FPL, CPL>(P, S, p);
+    const SearchOut o = warp_beam_search<DT, MT, FPL, CPL, FASTF>(P, S, p);
     if (lane_id() == 0) {
       ra.stat_vis[b] = o.vis_n;
       if (ra.stat_cmps) ra.stat_cmps[b] = o.cmps;
@@ -230,7 +236,9 @@ LaunchPlan plan_query(const IndexView& ix, const WarpLayout& lay, uint32_t Lmax)
 
 LaunchPlan plan_search(const IndexView& ix, const WarpLayout& lay, uint32_t L) {
   LaunchPlan p{1, 1};
-#define CALL4(DT, MT, F, C) p = plan_warp_kernel(k_search<DT, MT, F, C>, lay.total);
+#define CALL4(DT, MT, F, C)                                                          \
+  p = lay.fastf ? plan_warp_kernel(k_search<DT, MT, F, C, true>, lay.total)          \
+                : plan_warp_kernel(k_search<DT, MT, F, C, false>, lay.total);
 #define CALL(DT, MT) DD_DISPATCH_FC(L, ix.Rp, DT, MT, CALL4)
   DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
 #undef CALL
@@ -241,7 +249,9 @@ LaunchPlan plan_search(const IndexView& ix, const WarpLayout& lay, uint32_t L) {
 std::vector<LaunchPlan> search_plan_candidates(const IndexView& ix, const WarpLayout& lay,
                                                uint32_t L) {
   std::vector<LaunchPlan> v;
-#define CALL4(DT, MT, F, C) v = warp_kernel_candidates(k_search<DT, MT, F, C>, lay.total);
+#define CALL4(DT, MT, F, C)                                                          \
+  v = lay.fastf ? warp_kernel_candidates(k_search<DT, MT, F, C, true>, lay.total)    \
+                : warp_kernel_candidates(k_search<DT, MT, F, C, false>, lay.total);
 #define CALL(DT, MT) DD_DISPATCH_FC(L, ix.Rp, DT, MT, CALL4)
   DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
 #undef CALL
@@ -252,12 +262,15 @@ std::vector<LaunchPlan> search_plan_candidates(const IndexView& ix, const WarpLa
 void launch_search(const IndexView& ix, const RoundArgs& ra, const WarpLayout& lay,
                    const LaunchPlan& plan, int grid, cudaStream_t st) {
   const size_t sm = (size_t)lay.total * plan.warps_per_cta;
+#define CALL5(DT, MT, F, C, X)                                                       \
+  set_smem(k_search<DT, MT, F, C, X>, sm);                                           \
+  k_search<DT, MT, F, C, X><<<grid, plan.warps_per_cta * 32, sm, st>>>(ix, ra, lay);
 #define CALL4(DT, MT, F, C)                                                          \
-  set_smem(k_search<DT, MT, F, C>, sm);                                              \
-  k_search<DT, MT, F, C><<<grid, plan.warps_per_cta * 32, sm, st>>>(ix, ra, lay);
+  if (lay.fastf) { CALL5(DT, MT, F, C, true); } else { CALL5(DT, MT, F, C, false); }
 #define CALL(DT, MT) DD_DISPATCH_FC(ra.L, ix.Rp, DT, MT, CALL4)
   DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
 #undef CALL
+#undef CALL5
 #undef CALL4
 }
 

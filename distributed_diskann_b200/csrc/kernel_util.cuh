@@ -84,10 +84,13 @@ static int occupancy(K kernel, int threads, size_t smem) {
 template <typename K>
 static LaunchPlan plan_warp_kernel(K kernel, uint32_t bytes_per_warp) {
   LaunchPlan best{1, 0};
-  static const int cand[] = {1, 2, 4, 5, 8, 16};
+  static const int cand[] = {1, 2, 4, 5, 7, 8, 11, 16};
+  cudaFuncAttributes fa{};
+  const int max_threads =
+      cudaFuncGetAttributes(&fa, kernel) == cudaSuccess ? fa.maxThreadsPerBlock : 512;
   for (int wpc : cand) {
     const size_t sm = (size_t)bytes_per_warp * wpc;
-    if (sm > 227 * 1024) break;
+    if (sm > 227 * 1024 || wpc * 32 > max_threads) break;
     const int b = occupancy(kernel, wpc * 32, sm);
     if (b * wpc > best.warps_per_cta * best.blocks_per_sm) best = LaunchPlan{wpc, b};
   }
@@ -95,15 +98,19 @@ static LaunchPlan plan_warp_kernel(K kernel, uint32_t bytes_per_warp) {
   return best;
 }
 
-// The CTA shapes the autotuner times for a per-warp kernel: 2, 4, 8 and 16
-// warps per CTA, each with the CTAs per SM the occupancy API allows.
+// The CTA shapes the autotuner times for a per-warp kernel: 2, 4, 7, 8, 11
+// and 16 warps per CTA (within the kernel's launch bounds), each with the
+// CTAs per SM the occupancy API allows.
 template <typename K>
 static std::vector<LaunchPlan> warp_kernel_candidates(K kernel, uint32_t bytes_per_warp) {
   std::vector<LaunchPlan> v;
-  static const int cand[] = {2, 4, 8, 16};
+  static const int cand[] = {2, 4, 7, 8, 11, 16};
+  cudaFuncAttributes fa{};
+  const int max_threads =
+      cudaFuncGetAttributes(&fa, kernel) == cudaSuccess ? fa.maxThreadsPerBlock : 512;
   for (int wpc : cand) {
     const size_t sm = (size_t)bytes_per_warp * wpc;
-    if (sm > 227 * 1024) break;
+    if (sm > 227 * 1024 || wpc * 32 > max_threads) break;
     const int b = occupancy(kernel, wpc * 32, sm);
     if (b >= 1) v.push_back(LaunchPlan{wpc, b});
   }

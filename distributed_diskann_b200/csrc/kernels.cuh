@@ -19,6 +19,7 @@ struct WarpLayout {
   uint32_t hbits;  // hash bits of the largest beam width of the launch
   uint32_t h24;    // hash table of 24-bit ids (every id < 0xFFFFFF)
   uint32_t keep_vis;  // query layout holds the visited list (debug beam search)
+  uint32_t fastf;     // build search with the fast form's seen filter (16-bit tags)
 };
 
 // Per-warp shared-memory carve-up of k_prune (byte offsets, 16-byte aligned).
@@ -45,8 +46,9 @@ struct IndexView {
 
 // keep_vis: the query layout reserves the visited list (k_beam keeps it;
 // k_query only needs the evicted list)
+// fastf (build only): the fast form's seen filter, 16-bit tags (search_core.cuh)
 WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, uint32_t vcap,
-                              bool build, bool h24, bool keep_vis = true);
+                              bool build, bool h24, bool keep_vis = true, bool fastf = false);
 // tensor: the fast form's tensor-core greedy (integer data); false: the plain form
 PruneLayout make_prune_layout(uint32_t d, int dtype, uint32_t Rp, uint32_t ccap, bool tensor);
 

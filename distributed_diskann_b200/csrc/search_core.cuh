@@ -56,6 +56,34 @@ __host__ __device__ inline uint32_t hash_table_bytes(uint32_t hbits, bool h24) {
   return (h24 ? 3u : 4u) << hbits;
 }
 
+// ---------------------------------------------------------------------------
+// The fast form's "seen" filter (build searches of single-pass builds with
+// every id below 2^24 - 1).  In a build search (k = 0, no k-cut) the filter
+// only decides which neighbours get their distance computed: an id it lets
+// through twice is re-evaluated, fails the cutoff or is already in the
+// frontier, and set_union drops the copy (graph rows of a single-pass build
+// hold no repeated id).  So any filter without false positives gives the
+// reference's frontier, visited list and graph; only the dist_cmps count
+// moves.  This one keeps 2^hbits slots like the reference's, but hashes ids
+// with a bijection of [0, 2^24) and stores the 24 - hbits quotient bits in a
+// 16-bit tag: 2 bytes a slot instead of 3, and a lookup + insert with no
+// same-slot grouping (all lanes read their slots, then the lanes that
+// missed write: a lane that loses a write race only causes a later
+// re-evaluation).
+// ---------------------------------------------------------------------------
+__host__ __device__ inline uint32_t fast_table_bytes(uint32_t hbits) { return 2u << hbits; }
+
+// bijective mix of a 24-bit id (xor-shifts and odd multipliers mod 2^24)
+__device__ __forceinline__ uint32_t mix24(uint32_t x) {
+  x &= 0xFFFFFFu;
+  x ^= x >> 12;
+  x = (x * 0x9E3779u) & 0xFFFFFFu;
+  x ^= x >> 11;
+  x = (x * 0x85EBCBu) & 0xFFFFFFu;
+  x ^= x >> 12;
+  return x;
+}
+
 // the id a slot holds (DD_NONE when empty); h24 is warp-uniform
 __device__ __forceinline__ uint32_t hash_get(const SearchSmem& S, uint32_t nslots, uint32_t slot) {
   if (S.h24) {
@@ -133,17 +161,20 @@ __device__ __forceinline__ float point_dist(const SearchParams& P, const uint8_t
 // self_id: the id the reference skips as p.id() (the point itself in the
 // build, the query's index in searchAll).
 // FPL: frontier entries per lane (L <= 32*FPL); CPL: 32-lane chunks of a row (Rp <= 32*CPL).
-template <int DT, int MT, int FPL, int CPL>
+// FASTF: the fast form's seen filter (see fast_table_bytes), build searches only.
+template <int DT, int MT, int FPL, int CPL, bool FASTF = false>
 __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S, uint64_t self_id) {
   const uint32_t lane = lane_id();
   const uint32_t FULL = 0xffffffffu;
   const uint32_t nslots = 1u << P.hbits;
   const uint32_t hmask = nslots - 1;
   {
-    // all-ones bytes are the empty marker of both layouts
+    // all-ones bytes are the empty marker of every layout (a 16-bit tag of
+    // the fast filter is below 2^14)
     uint4* h4 = (uint4*)S.hash;
     const uint4 none = make_uint4(DD_NONE, DD_NONE, DD_NONE, DD_NONE);
-    const uint32_t n16 = hash_table_bytes(P.hbits, S.h24 != 0) / 16u;
+    const uint32_t n16 =
+        (FASTF ? fast_table_bytes(P.hbits) : hash_table_bytes(P.hbits, S.h24 != 0)) / 16u;
     for (uint32_t i = lane; i < n16; i += 32) h4[i] = none;
   }
   if (lane == 0) {
@@ -234,7 +265,29 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
     // first (they do not depend on the table); the table is then read and
     // written chunk after chunk.
     bool keep[CPL];
-    {
+    if (FASTF) {
+      uint16_t* tab = (uint16_t*)S.hash;
+      uint32_t slot[CPL];
+      uint16_t tag[CPL];
+#pragma unroll
+      for (int t = 0; t < CPL; t++) {
+        uint32_t at = a[t];
+        if (at != DD_NONE && at >= P.n) {
+          dd_set_error(P.err, DD_EBAD_ID);
+          at = DD_NONE;
+          a[t] = DD_NONE;
+        }
+        const uint32_t f = mix24(at);
+        slot[t] = f & hmask;
+        tag[t] = (uint16_t)(f >> P.hbits);
+        keep[t] = (at != DD_NONE) && ((uint64_t)at != self_id) && tab[slot[t]] != tag[t];
+      }
+      __syncwarp();
+#pragma unroll
+      for (int t = 0; t < CPL; t++)
+        if (keep[t]) tab[slot[t]] = tag[t];
+      __syncwarp();
+    } else {
       bool part[CPL];
       uint32_t loc[CPL], grp[CPL], prev_a[CPL];
 #pragma unroll

@@ -51,16 +51,24 @@ def test_build_and_search_bit_exact_vs_reference(golden, name, mode):
 
 
 def test_build_stats_match_oracle(oracle_mod):
+    """The plain form replays the reference's lossy seen filter, so even its
+    dist_cmps count is the reference's.  The fast form's filter (16-bit tags of
+    a bijective hash) gives the same graph and visited lists; only the number
+    of re-evaluated neighbours, dist_cmps, may differ."""
     base, _ = case_inputs("i8_small")
-    gi, graph, st = gpu_build(base, 64, 128, 1.2)
     og, ost = oracle_mod.build(base, 64, 128, 1.2)
-    np.testing.assert_array_equal(graph, canon(og))
-    assert st["visited"] == ost["visited"]
-    assert st["dist_cmps"] == ost["dist_cmps"]
-    assert st["groups"] == ost["groups"]
-    assert st["reverse_prunes"] == ost["reverse_prunes"]
-    assert st["prune_cands"] == ost["prune_cands"]
-    gi.close()
+    for mode in ("plain", "fast"):
+        gi, graph, st = gpu_build(base, 64, 128, 1.2, mode=mode)
+        np.testing.assert_array_equal(graph, canon(og))
+        assert st["visited"] == ost["visited"]
+        if mode == "plain":
+            assert st["dist_cmps"] == ost["dist_cmps"]
+        else:
+            assert abs(st["dist_cmps"] / ost["dist_cmps"] - 1.0) < 0.05
+        assert st["groups"] == ost["groups"]
+        assert st["reverse_prunes"] == ost["reverse_prunes"]
+        assert st["prune_cands"] == ost["prune_cands"]
+        gi.close()
 
 
 def test_beam_search_frontier_and_visited_vs_reference(golden):
@@ -243,7 +251,7 @@ def test_32bit_hash_table_layout_matches_24bit(monkeypatch):
     out = []
     for flag in ("0", "1"):
         monkeypatch.setenv("DD_HASH32", flag)
-        gi, graph, st = gpu_build(base, 32, 64, 1.2)
+        gi, graph, st = gpu_build(base, 32, 64, 1.2, mode="plain")
         ids, _, vis, cm = gi.search(q, 10, [10, 50, 100, 200, 64] * 100)
         out.append((graph, st["visited"], st["dist_cmps"], ids, vis, cm))
         gi.close()
