@@ -38,7 +38,7 @@ class StatsC(C.Structure):
                 ("build_ms", dbl), ("search_prune_ms", dbl), ("reverse_ms", dbl),
                 ("search_ms", dbl), ("search_warps_per_cta", u32), ("prune_warps_per_cta", u32),
                 ("search_queue", C.c_int32), ("prune_queue", C.c_int32),
-                ("graph_replay", C.c_int32)]
+                ("graph_replay", C.c_int32), ("vcap", u32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -55,6 +55,7 @@ SIGNATURES = {
     "dd_check_errors": (i32, [vp]),
     "dd_upload_points": (i32, [vp, vp, u64]),
     "dd_upload_points_device": (i32, [vp, vp, u64]),
+    "dd_upload_points_async": (i32, [vp, vp, u64]),
     "dd_load_points_file": (i32, [vp, C.c_char_p]),
     "dd_upload_graph": (i32, [vp, vp]),
     "dd_download_graph": (i32, [vp, vp]),

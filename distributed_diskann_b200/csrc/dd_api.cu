@@ -118,10 +118,11 @@ void dfree(void* p) {
   if (p) cudaFree(p);
 }
 
-int check_error_word(dd_index* h) {
+int check_error_word(dd_index* h, uint32_t* bits = nullptr) {
   uint32_t e = 0;
   CK(cudaMemcpyAsync(&e, h->err, 4, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  if (bits) *bits = e;
   if (e) {
     cudaMemsetAsync(h->err, 0, 4, h->stream);
     std::string m = "device error:";
@@ -632,6 +633,20 @@ int dd_upload_points_device(dd_index* h, const void* rows, uint64_t row_stride_b
   return DD_OK;
 }
 
+int dd_upload_points_async(dd_index* h, const void* rows, uint64_t row_stride_bytes) {
+  if (!h || !rows) return DD_ERR_ARG;
+  uint64_t rb = (uint64_t)h->d * esize(h->dtype);
+  if (row_stride_bytes < rb) return fail(h, DD_ERR_ARG, "row stride %llu < row bytes %llu",
+                                         (unsigned long long)row_stride_bytes, (unsigned long long)rb);
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpy2DAsync(h->points, h->stride, rows, row_stride_bytes, rb, h->n,
+                       cudaMemcpyHostToDevice, h->stream));
+  return DD_OK;
+}
+
+// PointRange(char*) (include/utils/point_range.h:61-97): the file is read in
+// chunks into two pinned staging buffers; the upload of one chunk runs while
+// the next one is read from disk.
 int dd_load_points_file(dd_index* h, const char* path) {
   if (!h || !path) return DD_ERR_ARG;
   std::ifstream f(path, std::ios::binary);
@@ -640,11 +655,42 @@ int dd_load_points_file(dd_index* h, const char* path) {
   f.read((char*)hdr, 8);
   if (!f || hdr[0] != h->n || hdr[1] != h->d)
     return fail(h, DD_ERR_IO, "%s: header [%u, %u] does not match the index", path, hdr[0], hdr[1]);
-  uint64_t rb = (uint64_t)h->d * esize(h->dtype);
-  std::vector<char> buf(rb * h->n);
-  f.read(buf.data(), (std::streamsize)buf.size());
-  if (!f) return fail(h, DD_ERR_IO, "%s: truncated", path);
-  return dd_upload_points(h, buf.data(), rb);
+  CK(cudaSetDevice(h->device));
+  const uint64_t rb = (uint64_t)h->d * esize(h->dtype);
+  uint64_t chunk_bytes = 64ull << 20;  // DD_LOAD_CHUNK_BYTES overrides (tests use small chunks)
+  if (const char* e = getenv("DD_LOAD_CHUNK_BYTES")) chunk_bytes = std::max<uint64_t>(rb, atoll(e));
+  const uint64_t chunk_rows = std::max<uint64_t>(1, std::min<uint64_t>(h->n, chunk_bytes / rb));
+  char* stage[2] = {nullptr, nullptr};
+  cudaEvent_t done[2] = {nullptr, nullptr};
+  int rc = DD_OK;
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 2 && e == cudaSuccess; i++) {
+    e = cudaMallocHost((void**)&stage[i], chunk_rows * rb);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming);
+  }
+  for (uint64_t r0 = 0, c = 0; e == cudaSuccess && rc == DD_OK && r0 < h->n; r0 += chunk_rows, c++) {
+    const int b = (int)(c & 1);
+    const uint64_t rows = std::min<uint64_t>(chunk_rows, h->n - r0);
+    if (c >= 2) e = cudaEventSynchronize(done[b]);  // the upload that used this buffer ended
+    if (e != cudaSuccess) break;
+    f.read(stage[b], (std::streamsize)(rows * rb));
+    if (!f) {
+      rc = fail(h, DD_ERR_IO, "%s: truncated", path);
+      break;
+    }
+    e = cudaMemcpy2DAsync(h->points + r0 * h->stride, h->stride, stage[b], rb, rb, rows,
+                          cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(done[b], h->stream);
+  }
+  cudaError_t e2 = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = e2;
+  for (int i = 0; i < 2; i++) {
+    if (stage[i]) cudaFreeHost(stage[i]);
+    if (done[i]) cudaEventDestroy(done[i]);
+  }
+  if (rc) return rc;
+  CK(e);
+  return DD_OK;
 }
 
 int dd_upload_graph(dd_index* h, const uint32_t* rows) {
@@ -724,22 +770,21 @@ int dd_schedule(uint64_t n, uint64_t max_build, double max_fraction, int knn_mod
   return DD_OK;
 }
 
-int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
-  if (!h || !P) return DD_ERR_ARG;
-  if (P->L == 0 || P->L > kMaxL) return fail(h, DD_ERR_UNSUPPORTED, "L must be in [1, %u]", kMaxL);
+}  // extern "C"
+
+namespace {
+
+// One build with visited-list capacity vcap; *err_bits = the device error word.
+int build_once(dd_index* h, const dd_build_params* P, uint32_t vcap, dd_stats* stats,
+               uint32_t* err_bits) {
+  *err_bits = 0;
   uint32_t start = P->knn_mode ? 0 : P->start_point;  // include/index.h:127
-  if (start >= h->n) return fail(h, DD_ERR_ARG, "start point %u >= n", start);
-  if (!(P->alpha > 0)) return fail(h, DD_ERR_ARG, "alpha must be positive");
-  if (P->mode != DD_MODE_FAST && P->mode != DD_MODE_PLAIN)
-    return fail(h, DD_ERR_ARG, "mode must be DD_MODE_FAST or DD_MODE_PLAIN");
-  CK(cudaSetDevice(h->device));
   h->launches = 0;
   auto rounds = schedule(h->n, P->max_build, P->max_fraction, P->knn_mode);
   uint64_t Bmax = 1;
   for (auto& r : rounds) Bmax = std::max<uint64_t>(Bmax, r.second > r.first ? r.second - r.first : 0);
   int rc = ensure_build_scratch(h, Bmax);
   if (rc) return rc;
-  uint32_t vcap = P->vcap ? P->vcap : 4 * P->L;
   BuildPlan bp;
   bp.fast = P->mode == DD_MODE_FAST;
   // the fast form's seen filter needs ids below 2^24 and rows without repeats
@@ -836,7 +881,7 @@ int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
   }
   CK(cudaEventSynchronize(e1));
   CK(cudaGetLastError());
-  rc = check_error_word(h);
+  rc = check_error_word(h, err_bits);
   if (stats) {
     float ms = 0, ts = 0, tp = 0, tr = 0;
     cudaEventElapsedTime(&ms, e0, e1);
@@ -860,10 +905,46 @@ int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
     stats->search_queue = bp.fast && bp.squeue;
     stats->prune_queue = bp.fast && bp.pqueue;
     stats->graph_replay = use_graph;
+    stats->vcap = vcap;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
+  if (!h || !P) return DD_ERR_ARG;
+  if (P->L == 0 || P->L > kMaxL) return fail(h, DD_ERR_UNSUPPORTED, "L must be in [1, %u]", kMaxL);
+  uint32_t start = P->knn_mode ? 0 : P->start_point;  // include/index.h:127
+  if (start >= h->n) return fail(h, DD_ERR_ARG, "start point %u >= n", start);
+  if (!(P->alpha > 0)) return fail(h, DD_ERR_ARG, "alpha must be positive");
+  if (P->mode != DD_MODE_FAST && P->mode != DD_MODE_PLAIN)
+    return fail(h, DD_ERR_ARG, "mode must be DD_MODE_FAST or DD_MODE_PLAIN");
+  CK(cudaSetDevice(h->device));
+  // The reference's build searches have no visited-list limit (limit = n).
+  // Here each search keeps its visited list in a slice of vcap entries; when a
+  // search overflows it (the kernel flags it and the round goes on), the
+  // whole build is run again with twice the capacity, which gives the same
+  // graph (the build is deterministic), until the prune's shared memory for
+  // vcap + R candidates runs out.
+  uint32_t vcap = P->vcap ? P->vcap : 4 * P->L;
+  for (;;) {
+    uint32_t bits = 0;
+    int rc = build_once(h, P, vcap, stats, &bits);
+    if (rc == DD_ERR_DEVICE && bits == DD_EVIS_CAP && vcap < (1u << 20)) {
+      const uint32_t next = vcap * 2;
+      if (make_prune_layout(h->d, h->dtype, h->Rp, next + h->Rp, P->mode == DD_MODE_FAST).total >
+          227 * 1024)
+        return rc;
+      vcap = next;
+      continue;
+    }
+    return rc;
+  }
 }
 
 int dd_search_device(dd_index* h, const void* queries, uint64_t nq, uint64_t qstride,

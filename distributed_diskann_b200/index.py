@@ -111,6 +111,10 @@ class GpuIndex:
     def load_graph(self, path):
         self._ck(self.lib.dd_load_graph_file(self.h, os.fsencode(path)))
 
+    def load_points(self, path):
+        """Reads a reference .bin file ([u32 n][u32 d][rows]) into the index."""
+        self._ck(self.lib.dd_load_points_file(self.h, os.fsencode(path)))
+
     # ---------------------------------------------------------------- build
     def build(self, L_, alpha, max_fraction=1.0, max_build=0, start_point=0, two_pass=False,
               knn_mode=False, collect_stats=True, vcap=0, mode="fast") -> dict:

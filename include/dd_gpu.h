@@ -72,7 +72,8 @@ typedef struct dd_build_params {
   int32_t two_pass;      /* first pass with alpha = 1 ("two_pass"; knn_index semantics) */
   int32_t knn_mode;      /* 1: knn_index::build_index (max_fraction 1, sorted rows) */
   int32_t collect_stats; /* 1: fill visited / distance-count statistics */
-  uint32_t vcap;         /* visited-list capacity per search, 0 = 4 * L */
+  uint32_t vcap;         /* starting visited-list capacity per search (0 = 4 * L); it is
+                            doubled and the build rerun while a search overflows it */
   int32_t mode;          /* DD_MODE_FAST (0) or DD_MODE_PLAIN */
 } dd_build_params;
 
@@ -94,6 +95,7 @@ typedef struct dd_stats {
   int32_t search_queue;    /* 1: persistent searches fed by a device work queue */
   int32_t prune_queue;     /* 1: persistent prunes fed by a device work queue */
   int32_t graph_replay;    /* 1: the build ran as one replayed CUDA graph */
+  uint32_t vcap;           /* visited-list capacity the build ran with */
 } dd_stats;
 
 /* ------------------------------------------------------------------ handle */
@@ -116,7 +118,14 @@ int dd_check_errors(dd_index* h);
 /* PointRange: copies n rows of d elements; row_stride_bytes between rows */
 int dd_upload_points(dd_index* h, const void* rows, uint64_t row_stride_bytes);
 int dd_upload_points_device(dd_index* h, const void* rows, uint64_t row_stride_bytes);
-/* reads a reference .bin file ([u32 n][u32 d][n*d elements]) into the index */
+/* the same copy ordered on the handle's stream without waiting for it: rows
+ * should be pinned host memory (cudaMallocHost) for the copy to overlap other
+ * work, and must stay valid until the stream reaches the copy (any
+ * synchronizing call of the handle, or dd_check_errors) */
+int dd_upload_points_async(dd_index* h, const void* rows, uint64_t row_stride_bytes);
+/* reads a reference .bin file ([u32 n][u32 d][n*d elements]) into the index,
+ * through two pinned staging buffers: disk reads overlap the uploads
+ * (PointRange(char*), include/utils/point_range.h:61-97) */
 int dd_load_points_file(dd_index* h, const char* path);
 /* Graph rows in the reference layout: n rows of (R+1) uint32, row[0] = degree */
 int dd_upload_graph(dd_index* h, const uint32_t* rows);

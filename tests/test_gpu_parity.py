@@ -257,3 +257,47 @@ def test_32bit_hash_table_layout_matches_24bit(monkeypatch):
         gi.close()
     for a, b in zip(out[0], out[1]):
         np.testing.assert_array_equal(a, b)
+
+
+def test_load_points_file_builds_reference_graph(golden, tmp_path, monkeypatch):
+    """PointRange(char*): the reference's .bin file read through two pinned
+    staging buffers (small chunks here, so that the double buffering turns over
+    many times) gives the same points, hence the reference's graph."""
+    from distributed_diskann_b200._lib import DDError
+
+    g, _ = golden
+    base, _ = case_inputs("i8_small")
+    path = tmp_path / "base.bin"
+    D.write_bin(str(path), base)
+    monkeypatch.setenv("DD_LOAD_CHUNK_BYTES", str(64 * 1024))
+    gi = GpuIndex(base.dtype, "l2", base.shape[0], base.shape[1], 64)
+    gi.load_points(str(path))
+    gi.build(128, 1.2)
+    assert sha(canon(gi.graph())) == g["cases"]["i8_small"]["graph_sha256"]
+    gi.close()
+    # a header that does not match the index, and a truncated file
+    other = GpuIndex(base.dtype, "l2", base.shape[0] - 1, base.shape[1], 64)
+    with pytest.raises(DDError):
+        other.load_points(str(path))
+    other.close()
+    raw = path.read_bytes()
+    (tmp_path / "short.bin").write_bytes(raw[: len(raw) // 2])
+    gi = GpuIndex(base.dtype, "l2", base.shape[0], base.shape[1], 64)
+    with pytest.raises(DDError):
+        gi.load_points(str(tmp_path / "short.bin"))
+    gi.close()
+
+
+@pytest.mark.parametrize("mode", ["fast", "plain"])
+def test_visited_capacity_overflow_reruns_the_build(golden, mode):
+    """The reference's build searches keep every visited node; a visited-list
+    slice that overflows makes the build run again with twice the capacity,
+    so a tiny starting capacity still gives the reference's graph."""
+    g, _ = golden
+    base, _ = case_inputs("i8_small")
+    gi = GpuIndex(base.dtype, "l2", base.shape[0], base.shape[1], 64)
+    gi.upload_points(base)
+    st = gi.build(128, 1.2, vcap=8, mode=mode)
+    assert st["vcap"] > 128
+    assert sha(canon(gi.graph())) == g["cases"]["i8_small"]["graph_sha256"]
+    gi.close()
