@@ -63,6 +63,10 @@ SIGNATURES = {
     "dd_save_graph_file": (i32, [vp, C.c_char_p]),
     "dd_build": (i32, [vp, C.POINTER(BuildParamsC), C.POINTER(StatsC)]),
     "dd_schedule": (i32, [u64, u64, dbl, i32, vp, vp, u64, vp]),
+    "dd_shard_begin": (i32, [vp, C.POINTER(BuildParamsC), u64]),
+    "dd_shard_search_prune": (i32, [vp, u64, u64, vp]),
+    "dd_shard_apply_reverse": (i32, [vp, u64, u64, vp, i32, i32, vp, vp, u64, vp]),
+    "dd_shard_set_rows": (i32, [vp, vp, vp, u64]),
     "dd_search": (i32, [vp, vp, u64, u64, vp, u32, dbl, u64, u32, u32, i32, vp, vp, vp, vp]),
     "dd_search_device": (i32, [vp, vp, u64, u64, vp, u32, u32, dbl, u64, u32, u32, i32, vp, vp,
                                vp, vp]),

@@ -69,6 +69,10 @@ struct dd_index {
   uint64_t launches_per_graph = 0;
   uint32_t* qcls = nullptr;  // query class lists, counts and queues (fast search form)
   uint64_t qcls_words = 0;
+  // sharded build: the launch shapes and parameters set by dd_shard_begin
+  bool shard_ready = false;
+  dd_build_params shard_params{};
+  uint64_t shard_bmax = 0;
   std::vector<uint64_t> graph_key;  // what the captured graph was built for
 };
 
@@ -945,6 +949,140 @@ int dd_build(dd_index* h, const dd_build_params* P, dd_stats* stats) {
     }
     return rc;
   }
+}
+
+// ---------------------------------------------------------------- sharded build
+// One rank's share of each round of a build spread over P ranks, one GPU each,
+// every rank holding the whole graph (src/bsp_index.hpp:141-434): the batch is
+// split into P contiguous slices (:247-252) that the ranks search and prune;
+// the new rows are exchanged; each rank runs the reverse edges of the targets
+// it owns (t % P == rank, :362-373) and the changed rows are exchanged again.
+// Each step gives the same rows as the single-GPU build, so the sharded build
+// gives its graph.  The exchanges are the caller's (NCCL all-gathers).
+
+namespace {
+BuildPlan shard_plan(dd_index* h) {
+  const dd_build_params* P = &h->shard_params;
+  const uint32_t vcap = P->vcap ? P->vcap : 8 * P->L;
+  BuildPlan bp;
+  bp.fast = P->mode == DD_MODE_FAST;
+  const bool fastf = bp.fast && use_h24(h);
+  bp.slay = make_search_layout(h->d, h->dtype, P->L, h->Rp, vcap, true, use_h24(h), true, fastf);
+  bp.play = make_prune_layout(h->d, h->dtype, h->Rp, bp.slay.ccap, bp.fast);
+  bp.splan = plan_search(view(h), bp.slay, P->L);
+  bp.pplan = plan_prune(view(h), bp.play, bp.fast);
+  bp.squeue = bp.pqueue = bp.fast;
+  return bp;
+}
+
+RoundArgs shard_round_args(dd_index* h, uint64_t floor, uint64_t B, uint32_t* rows) {
+  RoundArgs ra;
+  ra.floor = floor;
+  ra.B = (uint32_t)B;
+  ra.L = h->shard_params.L;
+  ra.alpha = h->shard_params.alpha;
+  ra.start = h->shard_params.start_point;
+  ra.new_out = rows;
+  ra.stat_vis = h->stat_vis;
+  ra.stat_cmps = h->stat_cmps;
+  ra.vis_all = h->vis_all;
+  ra.qsearch = nullptr;
+  ra.qprune = nullptr;
+  return ra;
+}
+}  // namespace
+
+int dd_shard_begin(dd_index* h, const dd_build_params* P, uint64_t max_batch) {
+  if (!h || !P) return DD_ERR_ARG;
+  if (P->L == 0 || P->L > kMaxL) return fail(h, DD_ERR_UNSUPPORTED, "L must be in [1, %u]", kMaxL);
+  if (P->two_pass || P->knn_mode)
+    return fail(h, DD_ERR_UNSUPPORTED, "the sharded build is the single-pass BSP build");
+  if (P->start_point >= h->n) return fail(h, DD_ERR_ARG, "start point >= n");
+  if (!(P->alpha > 0)) return fail(h, DD_ERR_ARG, "alpha must be positive");
+  if (P->mode != DD_MODE_FAST && P->mode != DD_MODE_PLAIN)
+    return fail(h, DD_ERR_ARG, "mode must be DD_MODE_FAST or DD_MODE_PLAIN");
+  if (max_batch == 0 || max_batch > h->n) return fail(h, DD_ERR_ARG, "bad max_batch");
+  CK(cudaSetDevice(h->device));
+  h->shard_params = *P;
+  h->shard_bmax = max_batch;
+  int rc = ensure_build_scratch(h, max_batch);
+  if (rc) return rc;
+  BuildPlan bp = shard_plan(h);
+  if (bp.slay.total > 227 * 1024 || bp.play.total > 227 * 1024)
+    return fail(h, DD_ERR_UNSUPPORTED, "shared memory of L=%u too large", P->L);
+  rc = ensure_vis_all(h, max_batch * 2ull * bp.slay.vcap);
+  if (rc) return rc;
+  rc = ensure_queues(h, 2);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(h->graph, 0xff, h->n * h->Rp * 4ull, h->stream));
+  CK(cudaMemsetAsync(h->err, 0, 4, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->shard_ready = true;
+  return DD_OK;
+}
+
+int dd_shard_search_prune(dd_index* h, uint64_t lo, uint64_t hi, uint32_t* rows) {
+  if (!h || !rows) return DD_ERR_ARG;
+  if (!h->shard_ready) return fail(h, DD_ERR_ARG, "dd_shard_begin first");
+  if (hi < lo || hi > h->n || hi - lo > h->shard_bmax) return fail(h, DD_ERR_ARG, "bad slice");
+  if (hi == lo) return DD_OK;
+  CK(cudaSetDevice(h->device));
+  BuildPlan bp = shard_plan(h);
+  RoundArgs ra = shard_round_args(h, lo, hi - lo, rows);
+  if (bp.fast) {
+    CK(cudaMemsetAsync(h->queues, 0, 8, h->stream));
+    ra.qsearch = h->queues;
+    ra.qprune = h->queues + 1;
+  }
+  IndexView ix = view(h);
+  launch_search(ix, ra, bp.slay, bp.splan, grid_for(bp.splan, ra.B, h->sm_count), h->stream);
+  launch_prune_round(ix, ra, bp.play, bp.slay.vcap, bp.pplan, grid_for(bp.pplan, ra.B, h->sm_count),
+                     bp.fast, h->stream);
+  CK(cudaGetLastError());
+  return check_error_word(h);
+}
+
+int dd_shard_apply_reverse(dd_index* h, uint64_t floor, uint64_t ceiling, const uint32_t* batch_rows,
+                           int rank, int world, uint32_t* ids_out, uint32_t* rows_out,
+                           uint64_t cap, uint64_t* count) {
+  if (!h || !batch_rows || !ids_out || !rows_out || !count) return DD_ERR_ARG;
+  if (!h->shard_ready) return fail(h, DD_ERR_ARG, "dd_shard_begin first");
+  if (world < 1 || rank < 0 || rank >= world) return fail(h, DD_ERR_ARG, "bad rank / world");
+  if (ceiling < floor || ceiling > h->n || ceiling - floor > h->shard_bmax)
+    return fail(h, DD_ERR_ARG, "bad round");
+  *count = 0;
+  if (ceiling == floor) return DD_OK;
+  CK(cudaSetDevice(h->device));
+  BuildPlan bp = shard_plan(h);
+  const uint64_t B = ceiling - floor;
+  RoundArgs ra = shard_round_args(h, floor, B, const_cast<uint32_t*>(batch_rows));
+  IndexView ix = view(h);
+  CK(cudaMemsetAsync(h->counters, 0, 8 * 4, h->stream));
+  launch_apply_rows(ix, ra, h->stream);
+  SemisortScratch ss = make_ss(h);
+  ss.world = (uint32_t)world;
+  ss.rank = (uint32_t)rank;
+  const int res = launch_semisort(batch_rows, B * h->Rp, h->n, ss, h->stream);
+  ReverseScratch rs = make_rs(h, res);
+  launch_reverse(ix, ra, rs, bp.fast, h->stream, h->sm_count);
+  launch_export_rows(ix, rs.st, rs.heads, h->counters, cap, ids_out, rows_out, h->stream);
+  CK(cudaGetLastError());
+  uint32_t c[2] = {0, 0};
+  CK(cudaMemcpyAsync(c, h->counters, 8, cudaMemcpyDeviceToHost, h->stream));
+  int rc = check_error_word(h);  // synchronizes
+  if (rc) return rc;
+  *count = c[1];
+  if (c[1] > cap) return fail(h, DD_ERR_ARG, "%u changed rows exceed the capacity %llu", c[1],
+                              (unsigned long long)cap);
+  return DD_OK;
+}
+
+int dd_shard_set_rows(dd_index* h, const uint32_t* ids, const uint32_t* rows, uint64_t count) {
+  if (!h || (count && (!ids || !rows))) return DD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  launch_set_rows(view(h), ids, rows, count, h->stream);
+  CK(cudaGetLastError());
+  return check_error_word(h);
 }
 
 int dd_search_device(dd_index* h, const void* queries, uint64_t nq, uint64_t qstride,

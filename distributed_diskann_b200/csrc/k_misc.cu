@@ -117,6 +117,58 @@ __global__ void k_gt_merge(const double* part_d, const uint32_t* part_i, uint64_
   }
 }
 
+// ============================================================ sharded build exchange
+// The targets whose rows the reverse-edge step of this rank changed (the
+// segment heads of the grouped pairs) and their new rows, for the other ranks.
+__global__ void k_export_rows(const uint32_t* graph, uint32_t Rp, const uint32_t* st,
+                              const uint32_t* heads, const uint32_t* counters, uint64_t cap,
+                              uint32_t* ids_out, uint32_t* rows_out) {
+  const uint32_t T = counters[1];
+  const uint32_t lane = lane_id();
+  for (uint64_t k = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < T && k < cap;
+       k += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
+    const uint32_t t = st[heads[k]];
+    if (lane == 0) ids_out[k] = t;
+    for (uint32_t j = lane; j < Rp; j += 32) rows_out[k * Rp + j] = graph[(uint64_t)t * Rp + j];
+  }
+}
+
+// rows received from the other ranks; ids are checked against n
+__global__ void k_set_rows(uint32_t* graph, uint64_t n, uint32_t Rp, const uint32_t* ids,
+                           const uint32_t* rows, uint64_t count, uint32_t* err) {
+  const uint32_t lane = lane_id();
+  for (uint64_t k = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < count;
+       k += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
+    const uint32_t t = ids[k];
+    if (t >= n) {
+      if (lane == 0) dd_set_error(err, DD_EBAD_ID);
+      continue;
+    }
+    for (uint32_t j = lane; j < Rp; j += 32) {
+      uint32_t a = rows[k * Rp + j];
+      if (a != DD_NONE && a >= n) {
+        dd_set_error(err, DD_EBAD_ID);
+        a = DD_NONE;
+      }
+      graph[(uint64_t)t * Rp + j] = a;
+    }
+  }
+}
+
+void launch_export_rows(const IndexView& ix, const uint32_t* st, const uint32_t* heads,
+                        const uint32_t* counters, uint64_t cap, uint32_t* ids_out,
+                        uint32_t* rows_out, cudaStream_t stream) {
+  k_export_rows<<<1184, 256, 0, stream>>>(ix.graph, ix.Rp, st, heads, counters, cap, ids_out,
+                                          rows_out);
+}
+
+void launch_set_rows(const IndexView& ix, const uint32_t* ids, const uint32_t* rows,
+                     uint64_t count, cudaStream_t stream) {
+  if (!count) return;
+  const int grid = (int)std::min<uint64_t>((count * 32 + 255) / 256, 65536);
+  k_set_rows<<<grid, 256, 0, stream>>>(ix.graph, ix.n, ix.Rp, ids, rows, count, ix.err);
+}
+
 // ============================================================ graph formats
 __global__ void k_to_ref_rows(const uint32_t* graph, uint64_t n, uint32_t R, uint32_t Rp,
                               uint32_t* out) {

@@ -194,6 +194,15 @@ void launch_groundtruth(const IndexView& ix, const uint8_t* queries, uint64_t qs
                         uint32_t k, uint32_t* ids, float* dists, double* part_d,
                         uint32_t* part_i, uint32_t nchunks, cudaStream_t st);
 
+// sharded build exchange: the rows of the targets this rank's reverse step
+// changed (segments of the grouped pairs, st/heads/counters as in
+// ReverseScratch), and the application of rows received from other ranks
+void launch_export_rows(const IndexView& ix, const uint32_t* st, const uint32_t* heads,
+                        const uint32_t* counters, uint64_t cap, uint32_t* ids_out,
+                        uint32_t* rows_out, cudaStream_t stream);
+void launch_set_rows(const IndexView& ix, const uint32_t* ids, const uint32_t* rows,
+                     uint64_t count, cudaStream_t stream);
+
 // graph format conversion (device rows <-> reference [deg, nbr...] rows)
 void launch_to_ref_rows(const IndexView& ix, uint32_t* out, cudaStream_t st);
 void launch_from_ref_rows(const IndexView& ix, const uint32_t* in, cudaStream_t st);

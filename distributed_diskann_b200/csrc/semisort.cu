@@ -59,10 +59,16 @@ static void gscan(uint32_t* a, uint64_t n_host, const uint32_t* n_dev, uint32_t*
 
 // ---- radix passes; the first pass reads new_out directly (key = index) and
 // drops empty slots
+// a slot of new_out the first pass keeps: filled, and owned by this rank
+__device__ __forceinline__ bool owned_pair(uint32_t t, uint32_t world, uint32_t rank) {
+  return t != DD_NONE && (world == 1 || t % world == rank);
+}
+
 __global__ void __launch_bounds__(kRadixThreads) k_radix_hist(const uint32_t* t_in,
                                                               const uint32_t* counters, uint64_t E,
                                                               int first, int shift, uint32_t G,
-                                                              uint32_t* hist) {
+                                                              uint32_t* hist, uint32_t world,
+                                                              uint32_t rank) {
   __shared__ uint32_t h[256];
   const uint32_t tid = threadIdx.x;
   h[tid] = 0;
@@ -73,7 +79,7 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_hist(const uint32_t* t_
     uint64_t i = base + (uint64_t)it * kRadixThreads + tid;
     if (i < len) {
       uint32_t t = t_in[i];
-      if (!first || t != DD_NONE) atomicAdd(&h[(t >> shift) & 255u], 1u);
+      if (!first || owned_pair(t, world, rank)) atomicAdd(&h[(t >> shift) & 255u], 1u);
     }
   }
   __syncthreads();
@@ -82,7 +88,8 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_hist(const uint32_t* t_
 
 __global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(
     const uint32_t* t_in, const uint32_t* v_in, const uint32_t* counters, uint64_t E, int first,
-    int shift, uint32_t G, const uint32_t* hist, uint32_t* t_out, uint32_t* v_out) {
+    int shift, uint32_t G, const uint32_t* hist, uint32_t* t_out, uint32_t* v_out,
+    uint32_t world, uint32_t rank) {
   __shared__ uint32_t run[256];
   __shared__ uint32_t boff[256];
   __shared__ uint32_t wcnt[kRadixThreads / 32][256];
@@ -101,7 +108,7 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(
     if (valid) {
       t = t_in[i];
       v = first ? (uint32_t)i : v_in[i];
-      if (first && t == DD_NONE) valid = false;
+      if (first && !owned_pair(t, world, rank)) valid = false;
     }
     const uint32_t dig = (t >> shift) & 255u;
     for (uint32_t d = lane; d < 256; d += 32) wcnt[warp][d] = 0;
@@ -153,10 +160,11 @@ int launch_semisort(const uint32_t* new_out, uint64_t E, uint64_t n, SemisortScr
   int cur = 0;
   for (int p = 0; p < passes; p++) {
     const int first = p == 0;
-    k_radix_hist<<<G, kRadixThreads, 0, st>>>(tin, s.counters, E, first, 8 * p, G, s.hist);
+    k_radix_hist<<<G, kRadixThreads, 0, st>>>(tin, s.counters, E, first, 8 * p, G, s.hist,
+                                              s.world, s.rank);
     gscan(s.hist, 256ull * G, nullptr, s.block_sums, first ? &s.counters[0] : nullptr, st);
     k_radix_scatter<<<G, kRadixThreads, 0, st>>>(tin, vin, s.counters, E, first, 8 * p, G, s.hist,
-                                                 s.t[cur], s.v[cur]);
+                                                 s.t[cur], s.v[cur], s.world, s.rank);
     tin = s.t[cur];
     vin = s.v[cur];
     cur ^= 1;

@@ -22,6 +22,9 @@ struct SemisortScratch {
   uint32_t* block_sums;
   uint32_t* counters;  // [0] valid pairs V, [1] segments T
   uint64_t cap;        // E
+  // owner filter of a sharded build: only targets t with t % world == rank
+  // are kept (world = 1: every target)
+  uint32_t world = 1, rank = 0;
 };
 
 // Sorts the valid entries of new_out (E = B*Rp, DD_NONE = empty slot) by

@@ -48,6 +48,7 @@ class GpuIndex:
 
     def __init__(self, dtype, metric, n, d, R, device=0):
         self.lib = L.load()
+        self.device = int(device)
         self.dtype = np.dtype(dtype)
         self.metric = metric
         self.n, self.d, self.R = int(n), int(d), int(R)

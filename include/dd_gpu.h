@@ -144,6 +144,31 @@ int dd_build(dd_index* h, const dd_build_params* params, dd_stats* stats);
 int dd_schedule(uint64_t n, uint64_t max_build, double max_fraction, int knn_mode,
                 uint64_t* floors, uint64_t* ceilings, uint64_t cap, uint64_t* nrounds);
 
+/* ------------------------------------------------------------------ sharded build
+ * One rank's steps of the build spread over P ranks, one GPU each, every rank
+ * holding the whole points and graph: BSP_index's superstep pair
+ * (src/bsp_index.hpp:238-407) with the MPI broadcasts of
+ * include/bsp/broadcast_bsp_framework.cpp:166-218 left to the caller (NCCL
+ * all-gathers of device buffers).  Per round [floor, ceiling) of dd_schedule:
+ *   1. dd_shard_search_prune on the rank's slice [lo, hi) of the batch
+ *      (slice r of P: floor + r*(B/P) + min(r, B%P), B/P + (r < B%P) points,
+ *      src/bsp_index.hpp:247-252): hi-lo new out-lists of dd_device_row_len
+ *      ids (padding 0xFFFFFFFF) into `rows` (device);
+ *   2. all-gather the slices into the batch's B rows, in batch order;
+ *   3. dd_shard_apply_reverse: update_neighbors of the batch, then the reverse
+ *      edges of the targets this rank owns (t % P == rank, :362-373), append
+ *      or robustPrune; the changed targets' ids and rows go to ids_out /
+ *      rows_out (device, room for cap), their number to *count;
+ *   4. all-gather those and apply the other ranks' with dd_shard_set_rows.
+ * The result equals dd_build's graph.  Single-pass builds only (no two_pass,
+ * no knn_mode); vcap 0 means 8 * L here, and an overflow is an error. */
+int dd_shard_begin(dd_index* h, const dd_build_params* params, uint64_t max_batch);
+int dd_shard_search_prune(dd_index* h, uint64_t lo, uint64_t hi, uint32_t* rows);
+int dd_shard_apply_reverse(dd_index* h, uint64_t floor, uint64_t ceiling, const uint32_t* batch_rows,
+                           int rank, int world, uint32_t* ids_out, uint32_t* rows_out,
+                           uint64_t cap, uint64_t* count);
+int dd_shard_set_rows(dd_index* h, const uint32_t* ids, const uint32_t* rows, uint64_t count);
+
 /* ------------------------------------------------------------------ search */
 /* searchAll: nq queries (rows of d elements, qstride bytes apart) searched
  * from `start` with QueryParams(k, L_per_query[i], cut, limit, degree_limit);

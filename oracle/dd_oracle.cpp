@@ -265,77 +265,99 @@ std::vector<std::pair<uint64_t, uint64_t>> schedule(uint64_t m, uint64_t max_bat
   return rounds;
 }
 
+// ---------------------------------------------------------------- one round
+// New out-lists of the batch points [lo, hi) against the current graph
+// (src/bsp_index.hpp:259-277; include/index.h:274-285).
+std::vector<std::vector<id_t_>> search_prune_range(const Space& S, const GraphView& G, uint32_t L,
+                                                   double alpha, uint32_t start, uint64_t lo,
+                                                   uint64_t hi, int nthreads, uint64_t* st) {
+  const uint32_t R = G.R;
+  const size_t B = hi - lo;
+  std::vector<std::vector<id_t_>> new_out(B);
+  std::vector<uint64_t> vis_cnt(B), cmp_cnt(B);
+  parallel_for(0, B, nthreads, [&](size_t b) {
+    id_t_ idx = (id_t_)(lo + b);
+    BeamResult r = beam_search(S, G, S.row(idx), idx, start, 0, L, 0.0, (int64_t)S.n,
+                               (int64_t)R);
+    vis_cnt[b] = r.visited.size();
+    cmp_cnt[b] = r.dist_cmps;
+    new_out[b] = robust_prune(S, G, idx, r.visited, alpha, R);
+  });
+  if (st)
+    for (size_t b = 0; b < B; b++) st[1] += vis_cnt[b], st[2] += cmp_cnt[b];
+  return new_out;
+}
+
+// update_neighbors of the batch [floor_, floor_ + B) (:354-357), then the
+// reverse edges of the targets t with t % world == rank (:362-407): flatten
+// (target, source) in batch order, group by target keeping the input order
+// within a target (parlay group_by_key), append or prune.  Returns the
+// changed targets in ascending order.
+std::vector<id_t_> apply_reverse_owned(const Space& S, GraphView& G, double alpha, uint64_t floor_,
+                                       const std::vector<std::vector<id_t_>>& new_out,
+                                       uint32_t rank, uint32_t world, int nthreads, uint64_t* st) {
+  const uint32_t R = G.R;
+  const size_t B = new_out.size();
+  for (size_t b = 0; b < B; b++) {
+    uint32_t* row = G.row(floor_ + b);
+    row[0] = (uint32_t)new_out[b].size();
+    for (size_t j = 0; j < new_out[b].size(); j++) row[1 + j] = new_out[b][j];
+  }
+  std::vector<std::pair<id_t_, id_t_>> pairs;
+  for (size_t b = 0; b < B; b++)
+    for (id_t_ t : new_out[b])
+      if (t % world == rank) pairs.push_back({t, (id_t_)(floor_ + b)});
+  std::stable_sort(pairs.begin(), pairs.end(),
+                   [](const std::pair<id_t_, id_t_>& a, const std::pair<id_t_, id_t_>& b) {
+                     return a.first < b.first;
+                   });
+  std::vector<size_t> seg;
+  for (size_t i = 0; i < pairs.size(); i++)
+    if (i == 0 || pairs[i].first != pairs[i - 1].first) seg.push_back(i);
+  seg.push_back(pairs.size());
+  size_t ngroups = seg.size() - 1;
+  std::vector<uint8_t> pruned(ngroups, 0);
+  std::vector<uint64_t> pc(ngroups, 0);
+  parallel_for(0, ngroups, nthreads, [&](size_t gi) {
+    id_t_ t = pairs[seg[gi]].first;
+    size_t m = seg[gi + 1] - seg[gi];
+    uint32_t* row = G.row(t);
+    if (m + row[0] <= R) {
+      for (size_t j = 0; j < m; j++) row[1 + row[0] + j] = pairs[seg[gi] + j].second;
+      row[0] += (uint32_t)m;
+    } else {
+      std::vector<pid> cc;
+      for (size_t j = 0; j < m; j++) {
+        id_t_ c = pairs[seg[gi] + j].second;
+        cc.push_back(pid(c, S.dist_ids(c, t)));  // wrapper :536-545
+      }
+      pc[gi] = m + row[0];
+      std::vector<id_t_> nn = robust_prune(S, G, t, cc, alpha, R);
+      row[0] = (uint32_t)nn.size();
+      for (size_t j = 0; j < nn.size(); j++) row[1 + j] = nn[j];
+      pruned[gi] = 1;
+    }
+  });
+  if (st) {
+    st[3] += ngroups;
+    for (size_t gi = 0; gi < ngroups; gi++) st[4] += pruned[gi], st[5] += pc[gi];
+  }
+  std::vector<id_t_> changed(ngroups);
+  for (size_t gi = 0; gi < ngroups; gi++) changed[gi] = pairs[seg[gi]].first;
+  return changed;
+}
+
 // ---------------------------------------------------------------- one pass
 // include/index.h:250-325 / src/bsp_index.hpp:238-407 with identity order.
 void batch_insert(const Space& S, GraphView& G, uint32_t L, double alpha, uint32_t start,
                   const std::vector<std::pair<uint64_t, uint64_t>>& rounds, int nthreads,
                   uint64_t* st) {
-  const uint32_t R = G.R;
   for (auto& rd : rounds) {
     uint64_t floor_ = rd.first, ceiling = rd.second;
     if (st) st[0]++;
     if (ceiling <= floor_) continue;
-    size_t B = ceiling - floor_;
-    std::vector<std::vector<id_t_>> new_out(B);
-    std::vector<uint64_t> vis_cnt(B), cmp_cnt(B);
-    // search + prune against the round-start snapshot (:259-277)
-    parallel_for(0, B, nthreads, [&](size_t b) {
-      id_t_ idx = (id_t_)(floor_ + b);
-      BeamResult r = beam_search(S, G, S.row(idx), idx, start, 0, L, 0.0, (int64_t)S.n,
-                                 (int64_t)R);
-      vis_cnt[b] = r.visited.size();
-      cmp_cnt[b] = r.dist_cmps;
-      new_out[b] = robust_prune(S, G, idx, r.visited, alpha, R);
-    });
-    if (st)
-      for (size_t b = 0; b < B; b++) st[1] += vis_cnt[b], st[2] += cmp_cnt[b];
-    // update_neighbors for the batch (:354-357)
-    for (size_t b = 0; b < B; b++) {
-      uint32_t* row = G.row(floor_ + b);
-      row[0] = (uint32_t)new_out[b].size();
-      for (size_t j = 0; j < new_out[b].size(); j++) row[1 + j] = new_out[b][j];
-    }
-    // flatten (target, source) in batch order, group by target keeping the
-    // input order within a target (:362-376; parlay group_by_key)
-    std::vector<std::pair<id_t_, id_t_>> pairs;
-    for (size_t b = 0; b < B; b++)
-      for (id_t_ t : new_out[b]) pairs.push_back({t, (id_t_)(floor_ + b)});
-    std::stable_sort(pairs.begin(), pairs.end(),
-                     [](const std::pair<id_t_, id_t_>& a, const std::pair<id_t_, id_t_>& b) {
-                       return a.first < b.first;
-                     });
-    std::vector<size_t> seg;
-    for (size_t i = 0; i < pairs.size(); i++)
-      if (i == 0 || pairs[i].first != pairs[i - 1].first) seg.push_back(i);
-    seg.push_back(pairs.size());
-    size_t ngroups = seg.size() - 1;
-    std::vector<uint8_t> pruned(ngroups, 0);
-    std::vector<uint64_t> pc(ngroups, 0);
-    // append or prune per target (:384-407)
-    parallel_for(0, ngroups, nthreads, [&](size_t gi) {
-      id_t_ t = pairs[seg[gi]].first;
-      size_t m = seg[gi + 1] - seg[gi];
-      uint32_t* row = G.row(t);
-      if (m + row[0] <= R) {
-        for (size_t j = 0; j < m; j++) row[1 + row[0] + j] = pairs[seg[gi] + j].second;
-        row[0] += (uint32_t)m;
-      } else {
-        std::vector<pid> cc;
-        for (size_t j = 0; j < m; j++) {
-          id_t_ c = pairs[seg[gi] + j].second;
-          cc.push_back(pid(c, S.dist_ids(c, t)));  // wrapper :536-545
-        }
-        pc[gi] = m + row[0];
-        std::vector<id_t_> nn = robust_prune(S, G, t, cc, alpha, R);
-        row[0] = (uint32_t)nn.size();
-        for (size_t j = 0; j < nn.size(); j++) row[1 + j] = nn[j];
-        pruned[gi] = 1;
-      }
-    });
-    if (st) {
-      st[3] += ngroups;
-      for (size_t gi = 0; gi < ngroups; gi++) st[4] += pruned[gi], st[5] += pc[gi];
-    }
+    auto new_out = search_prune_range(S, G, L, alpha, start, floor_, ceiling, nthreads, st);
+    apply_reverse_owned(S, G, alpha, floor_, new_out, 0, 1, nthreads, st);
   }
 }
 
@@ -404,6 +426,57 @@ int ddo_build(int dtype, int metric, const void* points, uint64_t n, uint32_t d,
         return S.dist_ids(i, j) < S.dist_ids(i, k);
       });
     });
+  }
+  return 0;
+}
+
+int ddo_shard_search_prune(int dtype, int metric, const void* points, uint64_t n, uint32_t d,
+                           uint64_t stride, const uint32_t* graph, uint32_t R, uint32_t L,
+                           double alpha, uint32_t start, uint64_t lo, uint64_t hi, int nthreads,
+                           uint32_t* rows_out) {
+  if (!points || !graph || !rows_out || hi < lo || hi > n || start >= n) return -1;
+  Space S = make_space(dtype, metric, points, n, d, stride);
+  GraphView G{const_cast<uint32_t*>(graph), R};
+  auto nb = search_prune_range(S, G, L, alpha, start, lo, hi, nthreads, nullptr);
+  for (size_t b = 0; b < nb.size(); b++) {
+    uint32_t* o = rows_out + b * (uint64_t)(R + 1);
+    std::memset(o, 0, 4ull * (R + 1));
+    o[0] = (uint32_t)nb[b].size();
+    for (size_t j = 0; j < nb[b].size(); j++) o[1 + j] = nb[b][j];
+  }
+  return 0;
+}
+
+int ddo_shard_apply_reverse(int dtype, int metric, const void* points, uint64_t n, uint32_t d,
+                            uint64_t stride, uint32_t* graph, uint32_t R, double alpha,
+                            uint64_t floor_, uint64_t ceiling, const uint32_t* batch_rows,
+                            uint32_t rank, uint32_t world, int nthreads, uint32_t* ids_out,
+                            uint32_t* rows_out, uint64_t cap, uint64_t* count) {
+  if (!points || !graph || !batch_rows || ceiling < floor_ || ceiling > n || world == 0 ||
+      rank >= world)
+    return -1;
+  Space S = make_space(dtype, metric, points, n, d, stride);
+  GraphView G{graph, R};
+  std::vector<std::vector<id_t_>> nb(ceiling - floor_);
+  for (size_t b = 0; b < nb.size(); b++) {
+    const uint32_t* r = batch_rows + b * (uint64_t)(R + 1);
+    nb[b].assign(r + 1, r + 1 + r[0]);
+  }
+  auto changed = apply_reverse_owned(S, G, alpha, floor_, nb, rank, world, nthreads, nullptr);
+  *count = changed.size();
+  if (changed.size() > cap) return -2;
+  for (size_t k = 0; k < changed.size(); k++) {
+    ids_out[k] = changed[k];
+    std::memcpy(rows_out + k * (uint64_t)(R + 1), G.row(changed[k]), 4ull * (R + 1));
+  }
+  return 0;
+}
+
+int ddo_shard_set_rows(uint32_t* graph, uint64_t n, uint32_t R, const uint32_t* ids,
+                       const uint32_t* rows, uint64_t count) {
+  for (uint64_t k = 0; k < count; k++) {
+    if (ids[k] >= n) return -1;
+    std::memcpy(graph + ids[k] * (uint64_t)(R + 1), rows + k * (uint64_t)(R + 1), 4ull * (R + 1));
   }
   return 0;
 }

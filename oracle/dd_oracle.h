@@ -30,6 +30,25 @@ int ddo_build(int dtype, int metric, const void* points, uint64_t n, uint32_t d,
               uint64_t max_build, uint32_t start, int two_pass, int knn_mode,
               int nthreads, uint32_t* graph_out, uint64_t* stats_out);
 
+/* One rank's steps of a round of the build spread over `world` ranks, every
+ * rank holding the whole graph (src/bsp_index.hpp:247-407): new out-lists of
+ * the batch slice [lo, hi) (rows_out, (hi-lo) x (R+1)); update_neighbors of
+ * the batch [floor, ceiling) from batch_rows, then the reverse edges of the
+ * targets t with t % world == rank, whose ids / new rows (ascending ids) go to
+ * ids_out / rows_out (room for cap rows; *count = their number); and the
+ * application of rows received from other ranks. */
+int ddo_shard_search_prune(int dtype, int metric, const void* points, uint64_t n, uint32_t d,
+                           uint64_t stride, const uint32_t* graph, uint32_t R, uint32_t L,
+                           double alpha, uint32_t start, uint64_t lo, uint64_t hi, int nthreads,
+                           uint32_t* rows_out);
+int ddo_shard_apply_reverse(int dtype, int metric, const void* points, uint64_t n, uint32_t d,
+                            uint64_t stride, uint32_t* graph, uint32_t R, double alpha,
+                            uint64_t floor_, uint64_t ceiling, const uint32_t* batch_rows,
+                            uint32_t rank, uint32_t world, int nthreads, uint32_t* ids_out,
+                            uint32_t* rows_out, uint64_t cap, uint64_t* count);
+int ddo_shard_set_rows(uint32_t* graph, uint64_t n, uint32_t R, const uint32_t* ids,
+                       const uint32_t* rows, uint64_t count);
+
 /* One beam_search (include/utils/beamSearch.h:51-184). graph is n x (R+1).
  * self_id is the id the search must skip (p.id() in the reference).
  * Returns 0, or -1 if an output buffer is too small. */

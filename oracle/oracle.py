@@ -67,6 +67,14 @@ def lib():
         L.ddo_groundtruth.argtypes = [i32, i32, vp, u64, u32, u64, vp, u64, u64, u32, i32, vp, vp]
         L.ddo_schedule.restype = u64
         L.ddo_schedule.argtypes = [u64, u64, dbl, i32, vp, vp, u64]
+        L.ddo_shard_search_prune.restype = i32
+        L.ddo_shard_search_prune.argtypes = [i32, i32, vp, u64, u32, u64, vp, u32, u32, dbl, u32,
+                                             u64, u64, i32, vp]
+        L.ddo_shard_apply_reverse.restype = i32
+        L.ddo_shard_apply_reverse.argtypes = [i32, i32, vp, u64, u32, u64, vp, u32, dbl, u64, u64,
+                                              vp, u32, u32, i32, vp, vp, u64, vp]
+        L.ddo_shard_set_rows.restype = i32
+        L.ddo_shard_set_rows.argtypes = [vp, u64, u32, vp, vp, u64]
         _lib = L
     return _lib
 
@@ -163,6 +171,51 @@ def groundtruth(points, queries, k, metric="l2", nthreads=0):
     lib().ddo_groundtruth(dt, METRICS[metric], _p(points), n, d, stride, _p(queries), nq,
                           queries.strides[0], k, int(nthreads), _p(ids), _p(ds))
     return ids, ds
+
+
+class ShardRankOracle:
+    """One rank of the sharded build on the CPU oracle (the per-round steps of
+    distributed_diskann_b200.sharded's protocol); rows in the reference layout
+    n x (R+1), row[0] = degree.  Test infrastructure, like the rest of this module."""
+
+    def __init__(self, points, R, L, alpha, metric="l2", start=0, nthreads=0):
+        self.points, self.dt, self.n, self.d, self.stride = _pts(points)
+        self.R, self.L, self.alpha, self.metric, self.start = R, L, alpha, metric, start
+        self.nthreads = nthreads
+        self.graph = np.zeros((self.n, R + 1), np.uint32)
+        self.row_len = R + 1
+
+    def search_prune(self, lo, hi):
+        rows = np.zeros((hi - lo, self.R + 1), np.uint32)
+        rc = lib().ddo_shard_search_prune(self.dt, METRICS[self.metric], _p(self.points), self.n,
+                                          self.d, self.stride, _p(self.graph), self.R, self.L,
+                                          float(self.alpha), self.start, lo, hi, self.nthreads,
+                                          _p(rows))
+        if rc != 0:
+            raise ValueError("oracle shard search/prune failed")
+        return rows
+
+    def apply_reverse(self, floor, ceiling, batch_rows, rank, world):
+        batch_rows = np.ascontiguousarray(batch_rows, np.uint32)
+        cap = batch_rows.shape[0] * self.R + 1
+        ids = np.zeros(cap, np.uint32)
+        rows = np.zeros((cap, self.R + 1), np.uint32)
+        cnt = np.zeros(1, np.uint64)
+        rc = lib().ddo_shard_apply_reverse(self.dt, METRICS[self.metric], _p(self.points), self.n,
+                                           self.d, self.stride, _p(self.graph), self.R,
+                                           float(self.alpha), floor, ceiling, _p(batch_rows), rank,
+                                           world, self.nthreads, _p(ids), _p(rows), cap, _p(cnt))
+        if rc != 0:
+            raise ValueError("oracle shard reverse failed")
+        c = int(cnt[0])
+        return ids[:c].copy(), rows[:c].copy()
+
+    def set_rows(self, ids, rows):
+        ids = np.ascontiguousarray(ids, np.uint32)
+        rows = np.ascontiguousarray(rows, np.uint32)
+        if lib().ddo_shard_set_rows(_p(self.graph), self.n, self.R, _p(ids), _p(rows),
+                                    len(ids)) != 0:
+            raise ValueError("bad row id")
 
 
 def schedule(n, max_build=0, xita=1.0, knn_mode=False):
