@@ -5,6 +5,7 @@
 //   k_to_ref_rows / k_from_ref_rows : device rows <-> the reference's
 //                     [deg, nbr...] rows (include/utils/graph.h:126-128)
 #include <cfloat>
+#include <climits>
 #include <cstdio>
 
 #include "dd_common.cuh"
@@ -92,6 +93,197 @@ __global__ void __launch_bounds__(256) k_gt_partial(IndexView ix, const uint8_t*
     uint64_t o = (q * nchunks + blockIdx.y) * k + lane;
     part_d[o] = bd;
     part_i[o] = bi;
+  }
+}
+
+// ---- integer data with rows of <= 128 bytes: the tensor cores.
+// d(q, p) = |q|^2 + |p|^2 - 2 q.p (L2) or -q.p (MIPS) with q.p from
+// mma.sync m16n8k32 (u8 x u8 / s8 x s8, s32 accumulation): exact integers,
+// the same values the CUDA-core form computes.  A CTA of two warps takes 32
+// queries (16 per warp: the A operand, kept in registers) against one chunk
+// of the base, streamed in tiles of 128 rows: cp.async copies the next tile
+// into shared memory (rows swizzled like the prune's Gram tiles) while the
+// warps multiply the current one.  Each (query, point) value is compared with
+// the query's k-th best; the few that pass are inserted, one warp-wide step
+// each, into the query's top-k list in shared memory.
+constexpr int kGtWarps = 2;
+constexpr int kGtQueries = 16 * kGtWarps;
+constexpr int kGtTile = 128;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
+
+// squared norm (L2) of a staged row of `words` 32-bit words, exact
+template <int DT>
+__device__ __forceinline__ int staged_norm(const uint32_t* rw, uint32_t r, uint32_t words) {
+  int acc = 0;
+  for (uint32_t q = 0; q < words; q++) {
+    const uint32_t v = mma_row_word(rw, r, q);
+    if (DT == DD_U8) acc = (int)__dp4a(v, v, (uint32_t)acc);
+    else acc = __dp4a((int)v, (int)v, acc);
+  }
+  return acc;
+}
+
+// (d, i) < (e, j) in the ground truth's order: distance, then id
+__device__ __forceinline__ bool gt_less(int d, uint32_t i, int e, uint32_t j) {
+  return d < e || (d == e && i < j);
+}
+
+// warp-wide insertion of (cd, ci) into the sorted list ld/li[0, k) (shared memory)
+__device__ __forceinline__ void gt_insert(int* ld, uint32_t* li, uint32_t k, int cd, uint32_t ci) {
+  const uint32_t lane = lane_id();
+  if (!gt_less(cd, ci, ld[k - 1], li[k - 1])) return;  // warp-uniform (same smem values)
+  const int d = lane < k ? ld[lane] : INT_MAX;
+  const uint32_t i = lane < k ? li[lane] : DD_NONE;
+  const bool before = lane < k && gt_less(d, i, cd, ci);
+  const uint32_t pos = __popc(__ballot_sync(0xffffffffu, before));
+  const int ud = __shfl_up_sync(0xffffffffu, d, 1);
+  const uint32_t ui = __shfl_up_sync(0xffffffffu, i, 1);
+  __syncwarp();
+  if (lane == pos) {
+    ld[lane] = cd;
+    li[lane] = ci;
+  } else if (lane > pos && lane < k) {
+    ld[lane] = ud;
+    li[lane] = ui;
+  }
+  __syncwarp();
+}
+
+template <int DT, int MT>
+__global__ void __launch_bounds__(kGtWarps * 32) k_gt_mma(IndexView ix, const uint8_t* queries,
+                                                          uint64_t qstride, uint64_t nq, uint32_t k,
+                                                          uint32_t nchunks, double* part_d,
+                                                          uint32_t* part_i) {
+  __shared__ __align__(16) uint32_t qrows[kGtQueries * 32];
+  __shared__ __align__(16) uint32_t tiles[2][kGtTile * 32];
+  __shared__ int tnorm[2][kGtTile];
+  __shared__ int top_d[kGtQueries][32];
+  __shared__ uint32_t top_i[kGtQueries][32];
+  const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
+  const uint32_t g = lane >> 2, t4 = lane & 3;
+  const uint64_t q0 = (uint64_t)blockIdx.x * kGtQueries;
+  const uint32_t words = (uint32_t)(ix.stride / 4);  // 16 or 32: rows of 64 or 128 bytes
+  const uint32_t KS = words / 8;                      // k-steps of 32 bytes
+  const uint64_t chunk = (ix.n + nchunks - 1) / nchunks;
+  const uint64_t c0 = (uint64_t)blockIdx.y * chunk;
+  const uint64_t c1 = min(ix.n, c0 + chunk);
+  for (uint32_t e = tid; e < kGtQueries * (words / 4); e += blockDim.x) {
+    const uint32_t r = e / (words / 4), w = e % (words / 4);
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (q0 + r < nq) v = __ldg((const uint4*)(queries + (q0 + r) * qstride) + w);
+    *mma_row_vec(qrows, r, w) = v;
+  }
+  for (uint32_t e = tid; e < kGtQueries * 32; e += blockDim.x) {
+    top_d[e / 32][e % 32] = INT_MAX;
+    top_i[e / 32][e % 32] = DD_NONE;
+  }
+  auto load_tile = [&](int buf, uint64_t base) {
+    for (uint32_t e = tid; e < kGtTile * (words / 4); e += blockDim.x) {
+      const uint32_t r = e / (words / 4), w = e % (words / 4);
+      if (base + r < c1)
+        cp_async16(mma_row_vec(tiles[buf], r, w), ix.points + (base + r) * ix.stride + 16 * w);
+      else
+        *mma_row_vec(tiles[buf], r, w) = make_uint4(0, 0, 0, 0);
+    }
+    cp_async_commit();
+  };
+  if (c0 < c1) load_tile(0, c0);
+  __syncthreads();
+  // A fragments of this warp's 16 queries (all k-steps) and their norms
+  const uint32_t ra = 16 * warp + g;
+  uint32_t afr[4][4];
+#pragma unroll
+  for (int ks = 0; ks < 4; ks++) {
+    const uint32_t qw = 8 * ks + t4;
+    const bool on = (uint32_t)ks < KS;
+    afr[ks][0] = on ? mma_row_word(qrows, ra, qw) : 0u;
+    afr[ks][1] = on ? mma_row_word(qrows, ra + 8, qw) : 0u;
+    afr[ks][2] = on ? mma_row_word(qrows, ra, qw + 4) : 0u;
+    afr[ks][3] = on ? mma_row_word(qrows, ra + 8, qw + 4) : 0u;
+  }
+  const int qn_lo = MT == DD_L2 ? staged_norm<DT>(qrows, ra, words) : 0;
+  const int qn_hi = MT == DD_L2 ? staged_norm<DT>(qrows, ra + 8, words) : 0;
+  const bool live_lo = q0 + ra < nq, live_hi = q0 + ra + 8 < nq;
+  // the k-th best of the rows g and g + 8 (refreshed after insertions)
+  int th_lo = INT_MAX, th_hi = INT_MAX;
+  uint32_t ti_lo = DD_NONE, ti_hi = DD_NONE;
+  int buf = 0;
+  for (uint64_t base = c0; base < c1; base += kGtTile, buf ^= 1) {
+    if (base + kGtTile < c1) {
+      load_tile(buf ^ 1, base + kGtTile);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    if (MT == DD_L2)
+      for (uint32_t r = tid; r < kGtTile; r += blockDim.x)
+        tnorm[buf][r] = staged_norm<DT>(tiles[buf], r, words);
+    __syncthreads();
+    const uint32_t* rw = tiles[buf];
+    for (int nt = 0; nt < kGtTile / 8; nt++) {
+      int acc[4] = {0, 0, 0, 0};
+      const uint32_t rb = 8 * nt + g;
+#pragma unroll
+      for (int ks = 0; ks < 4; ks++)
+        if ((uint32_t)ks < KS)
+          mma_k32<DT>(acc, afr[ks], mma_row_word(rw, rb, 8 * ks + t4),
+                      mma_row_word(rw, rb, 8 * ks + t4 + 4));
+      // acc[0..1]: query row g, points 8 nt + 2 t4 + {0, 1}; acc[2..3]: row g + 8
+      int dist[4];
+      uint32_t pass = 0;
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const uint32_t col = 8 * nt + 2 * t4 + (e & 1);
+        const bool lo = e < 2;
+        dist[e] = MT == DD_L2 ? (lo ? qn_lo : qn_hi) + tnorm[buf][col] - 2 * acc[e] : -acc[e];
+        const uint32_t pid = (uint32_t)(base + col);
+        if (base + col < c1 && (lo ? live_lo : live_hi) &&
+            gt_less(dist[e], pid, lo ? th_lo : th_hi, lo ? ti_lo : ti_hi))
+          pass |= 1u << e;
+      }
+      uint32_t anyp = __ballot_sync(0xffffffffu, pass != 0);
+      if (anyp) {
+        while (anyp) {
+          const int src = __ffs(anyp) - 1;
+          anyp &= anyp - 1;
+          const uint32_t m = __shfl_sync(0xffffffffu, pass, src);
+          int sd[4];
+#pragma unroll
+          for (int e = 0; e < 4; e++) sd[e] = __shfl_sync(0xffffffffu, dist[e], src);
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            if (m & (1u << e)) {
+              const uint32_t qr = 16 * warp + (uint32_t)(src >> 2) + (e < 2 ? 0u : 8u);
+              const uint32_t col = 8 * nt + 2 * (uint32_t)(src & 3) + (e & 1);
+              gt_insert(top_d[qr], top_i[qr], k, sd[e], (uint32_t)(base + col));
+            }
+          }
+        }
+        th_lo = top_d[ra][k - 1];
+        ti_lo = top_i[ra][k - 1];
+        th_hi = top_d[ra + 8][k - 1];
+        ti_hi = top_i[ra + 8][k - 1];
+      }
+    }
+    __syncthreads();  // the next iteration's copies overwrite this tile's buffer
+  }
+  for (uint32_t r = 0; r < 16; r++) {
+    const uint32_t qr = 16 * warp + r;
+    const uint64_t q = q0 + qr;
+    if (q < nq && lane < k) {
+      const uint64_t o = (q * nchunks + blockIdx.y) * k + lane;
+      const uint32_t id = top_i[qr][lane];
+      part_d[o] = id == DD_NONE ? INFINITY : (double)top_d[qr][lane];
+      part_i[o] = id;
+    }
   }
 }
 
@@ -210,14 +402,31 @@ __global__ void k_from_ref_rows(uint32_t* graph, uint64_t n, uint32_t R, uint32_
   }
 }
 
+bool groundtruth_uses_mma(const IndexView& ix) {
+  return ix.dtype != DD_F32 && (ix.stride == 64 || ix.stride == 128);
+}
+
 void launch_groundtruth(const IndexView& ix, const uint8_t* queries, uint64_t qstride, uint64_t nq,
                         uint32_t k, uint32_t* ids, float* dists, double* part_d, uint32_t* part_i,
                         uint32_t nchunks, cudaStream_t st) {
-  dim3 grid((unsigned)((nq + 7) / 8), nchunks);
+  if (groundtruth_uses_mma(ix)) {
+    // integer data of rows <= 128 bytes: tensor-core Gram tiles
+    dim3 grid((unsigned)((nq + kGtQueries - 1) / kGtQueries), nchunks);
+#define CALL(DT, MT)                                                                  \
+  k_gt_mma<DT, MT><<<grid, kGtWarps * 32, 0, st>>>(ix, queries, qstride, nq, k, nchunks, part_d, \
+                                                   part_i);
+    if (ix.dtype == DD_I8 && ix.metric == DD_L2) { CALL(DD_I8, DD_L2); }
+    else if (ix.dtype == DD_I8) { CALL(DD_I8, DD_MIPS); }
+    else if (ix.metric == DD_L2) { CALL(DD_U8, DD_L2); }
+    else { CALL(DD_U8, DD_MIPS); }
+#undef CALL
+  } else {
+    dim3 grid((unsigned)((nq + 7) / 8), nchunks);
 #define CALL(DT, MT)                                                                  \
   k_gt_partial<DT, MT><<<grid, 256, 0, st>>>(ix, queries, qstride, nq, k, nchunks, part_d, part_i);
-  DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
+    DD_DISPATCH_DM(ix.dtype, ix.metric, CALL);
 #undef CALL
+  }
   k_gt_merge<<<(unsigned)((nq + 7) / 8), 256, 0, st>>>(part_d, part_i, nq, k, nchunks, ids, dists);
 }
 

@@ -103,25 +103,32 @@ def test_robust_prune_vs_reference(golden):
     gi.close()
 
 
-@pytest.mark.parametrize("dtype,metric", [("f32", "l2"), ("f32", "mips"), ("i8", "l2"),
-                                          ("u8", "l2"), ("i8", "mips")])
-def test_groundtruth_vs_oracle(oracle_mod, dtype, metric):
+@pytest.mark.parametrize("dtype,metric,d", [("f32", "l2", 40), ("f32", "mips", 40),
+                                            ("i8", "l2", 40), ("u8", "l2", 40), ("i8", "mips", 40),
+                                            ("u8", "mips", 40), ("i8", "l2", 100),
+                                            ("u8", "l2", 128), ("u8", "l2", 200)])
+def test_groundtruth_vs_oracle(oracle_mod, dtype, metric, d):
+    """Brute force: FP64 for float data; integer rows of <= 128 bytes on the
+    tensor cores (exact int32 Gram tiles), wider ones on the CUDA cores.  Small
+    value ranges make many exact distance ties, which order by id."""
     rng = np.random.default_rng(7)
     if dtype == "f32":
-        base = rng.standard_normal((20_000, 40), dtype=np.float32)
-        q = rng.standard_normal((300, 40), dtype=np.float32)
+        base = rng.standard_normal((20_000, d), dtype=np.float32)
+        q = rng.standard_normal((300, d), dtype=np.float32)
     elif dtype == "i8":
-        base = rng.integers(-128, 128, (20_000, 40)).astype(np.int8)
-        q = rng.integers(-128, 128, (300, 40)).astype(np.int8)
+        base = rng.integers(-128, 128, (20_000, d)).astype(np.int8)
+        q = rng.integers(-128, 128, (300, d)).astype(np.int8)
     else:
-        base = rng.integers(0, 256, (20_000, 40)).astype(np.uint8)
-        q = rng.integers(0, 256, (300, 40)).astype(np.uint8)
+        hi = 256 if d != 128 else 3  # d = 128: values 0..2, ties everywhere
+        base = rng.integers(0, hi, (20_000, d)).astype(np.uint8)
+        q = rng.integers(0, hi, (300, d)).astype(np.uint8)
     gi = GpuIndex(base.dtype, metric, base.shape[0], base.shape[1], 8)
     gi.upload_points(base)
-    ids, ds = gi.groundtruth(q, 32)
-    oi, od = oracle_mod.groundtruth(base, q, 32, metric=metric)
-    np.testing.assert_array_equal(ids, oi)
-    np.testing.assert_array_equal(ds, od)
+    for k in (32, 10, 1):
+        ids, ds = gi.groundtruth(q, k)
+        oi, od = oracle_mod.groundtruth(base, q, k, metric=metric)
+        np.testing.assert_array_equal(ids, oi)
+        np.testing.assert_array_equal(ds, od)
     gi.close()
 
 
