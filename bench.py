@@ -345,7 +345,9 @@ def main():
     qres = None
     if not args.no_queries and rank == 0:
         k = 10
+        t_gt = time.time()
         gt_i, gt_d = gi.groundtruth(queries, 32)
+        t_gt = time.time() - t_gt
         tdt = {"u8": torch.uint8, "i8": torch.int8, "f32": torch.float32}[w.dtype]
         row_elems = int(gi.lib.dd_device_row_stride(gi.h)) // es
         qpad = torch.zeros((nq, row_elems), dtype=tdt, device=dev)  # padded device rows
@@ -366,7 +368,9 @@ def main():
 
         Lmix = torch.tensor(np.array(w.sweep_L, np.int32)[np.arange(nq) % len(w.sweep_L)],
                             device=dev)
-        qres = {"nq": nq, "k": k, "cut": 1.35}
+        qres = {"nq": nq, "k": k, "cut": 1.35,
+                "groundtruth_s": t_gt,  # host wall time of dd_groundtruth, k = 32, copies included
+                "groundtruth_form": "tensor-core Gram tiles" if w.dtype != "f32" else "FP64"}
         for form in ("fast", "plain"):
             gi.set_search_mode(form)
             sweep = []
