@@ -14,6 +14,7 @@
 #include "../../include/dd_gpu.h"
 #include "dd_common.cuh"
 #include "kernels.cuh"
+#include "search_core.cuh"
 #include "semisort.cuh"
 #include "sort_emul.cuh"
 
@@ -69,6 +70,8 @@ struct dd_index {
   uint64_t launches_per_graph = 0;
   uint32_t* qcls = nullptr;  // query class lists, counts and queues (fast search form)
   uint64_t qcls_words = 0;
+  uint32_t* qhash = nullptr;  // global seen tables of the wide beam-width classes
+  uint64_t qhash_words = 0;
   // sharded build: the launch shapes and parameters set by dd_shard_begin
   bool shard_ready = false;
   dd_build_params shard_params{};
@@ -586,6 +589,7 @@ int dd_destroy(dd_index* h) {
   for (void* p : ptrs) dfree(p);
   dfree(h->queues);
   dfree(h->qcls);
+  dfree(h->qhash);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
@@ -1121,6 +1125,7 @@ int dd_search_device(dd_index* h, const void* queries, uint64_t nq, uint64_t qst
   qa.cls_count = nullptr;
   qa.cls_queue = nullptr;
   qa.Lvalid = Lmax;
+  qa.hash_scratch = nullptr;
   if (h->search_mode == DD_MODE_PLAIN) {
     // one launch laid out for the largest beam width
     const LaunchPlan plan = plan_query(view(h), lay, Lmax);
@@ -1152,8 +1157,11 @@ int dd_search_device(dd_index* h, const void* queries, uint64_t nq, uint64_t qst
   for (int c = query_class(Lmax); c >= 0; c--) {
     if ((16u << c) < k && c < query_class(Lmax)) break;  // no valid beam width below k
     const uint32_t Lc = std::min<uint32_t>(16u << c, Lmax);
+    // seen tables above 16 KB (beam widths above 128) would cap the resident
+    // queries per SM by shared memory: they go to one global slice per warp
+    const bool hglob = hash_table_bytes(hash_bits_for(Lc), use_h24(h)) > 16384;
     WarpLayout lc = make_search_layout(h->d, h->dtype, Lc, h->Rp, 2 * Lc + 64, false,
-                                       use_h24(h), false);
+                                       use_h24(h), false, false, hglob);
     const LaunchPlan plan = plan_query(view(h), lc, Lc);
     QueryArgs qc = qa;
     qc.Lmax = Lc;
@@ -1163,6 +1171,17 @@ int dd_search_device(dd_index* h, const void* queries, uint64_t nq, uint64_t qst
     const int wpc = plan.warps_per_cta;
     const int grid = (int)std::min<uint64_t>((nq + wpc - 1) / wpc,
                                              (uint64_t)plan.blocks_per_sm * h->sm_count);
+    if (hglob) {
+      const uint64_t words = (uint64_t)grid * wpc * lc.hash_words;
+      if (words > h->qhash_words) {
+        dfree(h->qhash);
+        h->qhash = nullptr;
+        h->qhash_words = 0;
+        CK(dalloc(&h->qhash, words));
+        h->qhash_words = words;
+      }
+      qc.hash_scratch = h->qhash;
+    }
     launch_query(view(h), qc, lc, wpc, grid, h->stream);
     h->launches++;
   }

@@ -24,7 +24,7 @@ namespace ddk {
 // With h24 the hash table stores 24-bit ids (3 bytes a slot instead of 4),
 // which is exact whenever every id is below 0xFFFFFF.
 WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, uint32_t vcap,
-                              bool build, bool h24, bool keep_vis, bool fastf) {
+                              bool build, bool h24, bool keep_vis, bool fastf, bool hash_global) {
   WarpLayout w{};
   uint32_t esz = dtype == DD_F32 ? 4 : 1;
   uint32_t off = 0;
@@ -53,7 +53,9 @@ WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, ui
       w.vis_d = off; off += r16(4ull * vcap);
     }
     w.ws = off; off += r16(4ull * vcap);  // evicted list
-    off += hash_bytes;
+    w.hash_global = hash_global ? 1u : 0u;
+    w.hash_words = hash_bytes / 4;
+    if (!hash_global) off += hash_bytes;
   }
   w.total = r16(off);
   return w;
@@ -78,7 +80,8 @@ __device__ __forceinline__ SearchSmem carve_build(uint8_t* base, const WarpLayou
 }
 
 // query / debug layout: everything in shared memory
-__device__ __forceinline__ SearchSmem carve_query(uint8_t* base, const WarpLayout& w) {
+__device__ __forceinline__ SearchSmem carve_query(uint8_t* base, const WarpLayout& w,
+                                                  uint32_t* global_hash = nullptr) {
   SearchSmem S;
   S.qv = base + w.qv;
   S.fr_id = (uint32_t*)(base + w.fr_id);
@@ -90,7 +93,7 @@ __device__ __forceinline__ SearchSmem carve_query(uint8_t* base, const WarpLayou
   S.vis_id = w.keep_vis ? (uint32_t*)(base + w.vis_id) : nullptr;
   S.vis_d = w.keep_vis ? (float*)(base + w.vis_d) : nullptr;
   S.ev_id = (uint32_t*)(base + w.ws);
-  S.hash = (uint32_t*)(base + w.ws + r16(4ull * w.vcap));
+  S.hash = w.hash_global ? global_hash : (uint32_t*)(base + w.ws + r16(4ull * w.vcap));
   S.h24 = (int)w.h24;
   return S;
 }
@@ -139,7 +142,10 @@ __global__ void __launch_bounds__(512) k_query(IndexView ix, QueryArgs qa, WarpL
   extern __shared__ uint4 smem_raw[];
   const uint32_t wpc = blockDim.x >> 5, wic = threadIdx.x >> 5, lane = lane_id();
   const uint64_t gw = (uint64_t)blockIdx.x * wpc + wic;
-  const SearchSmem S = carve_query((uint8_t*)smem_raw + (size_t)wic * lay.total, lay);
+  // large seen tables (beam widths above 128) live in this warp's global slice
+  const SearchSmem S =
+      carve_query((uint8_t*)smem_raw + (size_t)wic * lay.total, lay,
+                  lay.hash_global ? qa.hash_scratch + gw * (uint64_t)lay.hash_words : nullptr);
   const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
   const uint64_t nitems = qa.cls_items ? (uint64_t)*qa.cls_count : qa.nq;
   uint64_t cur = gw;

@@ -20,6 +20,8 @@ struct WarpLayout {
   uint32_t h24;    // hash table of 24-bit ids (every id < 0xFFFFFF)
   uint32_t keep_vis;  // query layout holds the visited list (debug beam search)
   uint32_t fastf;     // build search with the fast form's seen filter (16-bit tags)
+  uint32_t hash_global;  // query layout: the seen table lives in a global slice per warp
+  uint32_t hash_words;   // its size in 32-bit words (16-byte multiple)
 };
 
 // Per-warp shared-memory carve-up of k_prune (byte offsets, 16-byte aligned).
@@ -47,8 +49,11 @@ struct IndexView {
 // keep_vis: the query layout reserves the visited list (k_beam keeps it;
 // k_query only needs the evicted list)
 // fastf (build only): the fast form's seen filter, 16-bit tags (search_core.cuh)
+// hash_global (query only): the seen table goes to a global slice per resident
+// warp (QueryArgs::hash_scratch) instead of shared memory
 WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, uint32_t vcap,
-                              bool build, bool h24, bool keep_vis = true, bool fastf = false);
+                              bool build, bool h24, bool keep_vis = true, bool fastf = false,
+                              bool hash_global = false);
 // tensor: the fast form's tensor-core greedy (integer data); false: the plain form
 PruneLayout make_prune_layout(uint32_t d, int dtype, uint32_t Rp, uint32_t ccap, bool tensor);
 
@@ -136,6 +141,7 @@ struct QueryArgs {
   const uint32_t* cls_count;
   uint32_t* cls_queue;
   uint32_t Lvalid;         // largest valid beam width (the caller's Lmax; Lmax is the class's)
+  uint32_t* hash_scratch;  // layouts with hash_global: one table per warp of the grid
 };
 
 // Beam-width classes of the bucketed query launch: class c serves beam widths
