@@ -56,6 +56,9 @@ def parse():
                     help="queries of the reference's timed query sweep")
     ap.add_argument("--plain-steps", type=int, default=3,
                     help="timed builds of the plain exact form (capped by --steps)")
+    ap.add_argument("--sharded", action="store_true",
+                    help="with N ranks: one build spread over the N GPUs (the reference's "
+                         "distributed build; NCCL all-gathers), instead of N independent builds")
     return ap.parse_args()
 
 
@@ -214,6 +217,73 @@ def D_recall(ids, gt_i, gt_d):
     return D.recall_with_ties(ids, gt_i, gt_d, 10)
 
 
+# ---------------------------------------------------------------------- sharded build
+def run_sharded(args, rank, world, local_rank):
+    """One build of the workload spread over the ranks (strong scaling): each
+    round's batch split by rank, reverse edges owned by target % N, two NCCL
+    all-gathers per round (distributed_diskann_b200/sharded.py)."""
+    import torch
+    import torch.distributed as dist
+
+    from distributed_diskann_b200 import datasets as D
+    from distributed_diskann_b200.index import GpuIndex
+    from distributed_diskann_b200.sharded import ShardRankGpu, TorchExchange, run_rank
+
+    dev = torch.device("cuda", local_rank)
+    w = D.WORKLOADS[args.workload]
+    n = args.n or w.n
+    base, _ = D.make_workload(w, n=n, nq=1)  # every rank holds the same points
+    base_t = torch.from_numpy(base).pin_memory()
+    gi = GpuIndex(base.dtype, w.metric, n, w.d, w.R, device=local_rank)
+    gi.upload_points(base)
+    sr = ShardRankGpu(gi, w.L, w.alpha, mode="fast", world=world)
+    ex = TorchExchange()
+    stream = torch.cuda.current_stream(dev)
+
+    def build():
+        sr.begin()
+        run_rank(sr, ex, rank, world, sr.rounds)
+
+    def timed(fn, steps):
+        dist.barrier()
+        torch.cuda.synchronize(dev)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            fn()
+        ev1.record(stream)
+        ev1.synchronize()
+        t = torch.tensor([ev0.elapsed_time(ev1) / 1000.0], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        build()
+    t = timed(build, args.steps)
+    graph_host = torch.empty((n, w.R + 1), dtype=torch.int32).pin_memory()
+
+    def e2e_step():
+        gi.lib.dd_upload_points(gi.h, base_t.data_ptr(), base_t.stride(0) * base_t.element_size())
+        build()
+        gi.lib.dd_download_graph(gi.h, graph_host.data_ptr())
+
+    t_e2e = timed(e2e_step, args.steps)
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": n * args.steps / t, "unit": "points/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": w.dtype,
+            "data": "synthetic",
+            "config": {"workload": f"{w.name}: {n}x{w.d} {w.dtype} {w.metric}, R={w.R}, L={w.L}, "
+                                   f"alpha={w.alpha} (one build spread over the GPUs)",
+                       "n": n, "parallelism": f"sharded build over {world} GPUs (NCCL all-gathers)",
+                       "l2_flush": "inputs larger than L2 (points + graph > 126 MB)"},
+            "e2e": {"value": n * args.steps / t_e2e, "unit": "points/s",
+                    "h2d_bytes_per_step": base.nbytes, "d2h_bytes_per_step": n * (w.R + 1) * 4},
+        }), flush=True)
+    gi.close()
+
+
 # ---------------------------------------------------------------------- our arm
 def main():
     args = parse()
@@ -232,10 +302,25 @@ def main():
     from distributed_diskann_b200.index import GpuIndex
 
     torch.cuda.set_device(local_rank)
-    if world > 1:
+    if world > 1 or args.sharded:
         from datetime import timedelta
 
+        if "MASTER_ADDR" not in os.environ:  # one rank outside torchrun
+            import socket
+
+            with socket.socket() as sk:
+                sk.bind(("127.0.0.1", 0))
+                os.environ["MASTER_PORT"] = str(sk.getsockname()[1])
+            os.environ["MASTER_ADDR"] = "127.0.0.1"
+            os.environ.setdefault("RANK", "0")
+            os.environ.setdefault("WORLD_SIZE", "1")
+
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    if args.sharded:
+        run_sharded(args, rank, world, local_rank)
+        dist.barrier()
+        dist.destroy_process_group()
+        return
     dev = torch.device("cuda", local_rank)
     w = D.WORKLOADS[args.workload]
     n = args.n or w.n

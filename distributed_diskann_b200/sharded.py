@@ -55,14 +55,18 @@ class ShardRankGpu:
         self.dev = torch.device("cuda", gi.device)
         self.row_len = int(gi.lib.dd_device_row_len(gi.h))
         self.rounds = schedule(gi.n, max_build, max_fraction)
-        bmax = max(1, max(c - f for f, c in self.rounds))
-        p = L.BuildParamsC(int(L_), float(alpha), float(max_fraction), int(max_build),
-                           int(start_point), 0, 0, 0, int(vcap), L.MODES[mode])
-        gi._ck(gi.lib.dd_shard_begin(gi.h, C.byref(p), bmax))
+        self.bmax = max(1, max(c - f for f, c in self.rounds))
+        self.params = L.BuildParamsC(int(L_), float(alpha), float(max_fraction), int(max_build),
+                                     int(start_point), 0, 0, 0, int(vcap), L.MODES[mode])
         # changed rows of one round: at most the targets this rank owns
-        self.cap = min(bmax * gi.R, -(-gi.n // world))
+        self.cap = min(self.bmax * gi.R, -(-gi.n // world))
         self.ids = torch.empty(self.cap, dtype=torch.int32, device=self.dev)
         self.rows = torch.empty((self.cap, self.row_len), dtype=torch.int32, device=self.dev)
+        self.begin()
+
+    def begin(self):
+        """Sets the launch shapes and empties the graph: the start of a build."""
+        self.gi._ck(self.gi.lib.dd_shard_begin(self.gi.h, C.byref(self.params), self.bmax))
 
     def search_prune(self, lo, hi):
         out = self.torch.empty((hi - lo, self.row_len), dtype=self.torch.int32, device=self.dev)
