@@ -72,6 +72,8 @@ struct dd_index {
   uint64_t qcls_words = 0;
   uint32_t* qhash = nullptr;  // global seen tables of the wide beam-width classes
   uint64_t qhash_words = 0;
+  uint32_t* qev = nullptr;    // evicted lists of the query searches
+  uint64_t qev_words = 0;
   // sharded build: the launch shapes and parameters set by dd_shard_begin
   bool shard_ready = false;
   dd_build_params shard_params{};
@@ -590,6 +592,7 @@ int dd_destroy(dd_index* h) {
   dfree(h->queues);
   dfree(h->qcls);
   dfree(h->qhash);
+  dfree(h->qev);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
@@ -1026,7 +1029,9 @@ int dd_shard_begin(dd_index* h, const dd_build_params* P, uint64_t max_batch) {
 }
 
 int dd_shard_search_prune(dd_index* h, uint64_t lo, uint64_t hi, uint32_t* rows) {
-  if (!h || !rows) return DD_ERR_ARG;
+  if (!h) return DD_ERR_ARG;
+  if (hi == lo) return DD_OK;  // an empty slice (batches smaller than the ranks)
+  if (!rows) return fail(h, DD_ERR_ARG, "rows is null");
   if (!h->shard_ready) return fail(h, DD_ERR_ARG, "dd_shard_begin first");
   if (hi < lo || hi > h->n || hi - lo > h->shard_bmax) return fail(h, DD_ERR_ARG, "bad slice");
   if (hi == lo) return DD_OK;
@@ -1126,12 +1131,32 @@ int dd_search_device(dd_index* h, const void* queries, uint64_t nq, uint64_t qst
   qa.cls_queue = nullptr;
   qa.Lvalid = Lmax;
   qa.hash_scratch = nullptr;
+  // Evicted lists (visited entries pushed out of the frontier, which a query
+  // must still treat as visited if they come back after a k-cut) live in a
+  // global slice per resident warp.  Their length is bounded by the visits
+  // of the search; ev_cap covers far more than any search here makes, and an
+  // overflow is reported through the error word (dd_check_errors).
+  qa.ev_cap = 4096 + 8 * Lmax;
+  auto ev_slices = [&](uint64_t warps) -> int {
+    const uint64_t words = warps * qa.ev_cap;
+    if (words > h->qev_words) {
+      dfree(h->qev);
+      h->qev = nullptr;
+      h->qev_words = 0;
+      CK(dalloc(&h->qev, words));
+      h->qev_words = words;
+    }
+    qa.ev_scratch = h->qev;
+    return DD_OK;
+  };
   if (h->search_mode == DD_MODE_PLAIN) {
     // one launch laid out for the largest beam width
     const LaunchPlan plan = plan_query(view(h), lay, Lmax);
     const int wpc = plan.warps_per_cta;
     const int grid = (int)std::min<uint64_t>((nq + wpc - 1) / wpc,
                                              (uint64_t)plan.blocks_per_sm * h->sm_count);
+    int rc = ev_slices((uint64_t)grid * wpc);
+    if (rc) return rc;
     launch_query(view(h), qa, lay, wpc, grid, h->stream);
     h->launches = 1;
     CK(cudaGetLastError());
@@ -1171,6 +1196,9 @@ int dd_search_device(dd_index* h, const void* queries, uint64_t nq, uint64_t qst
     const int wpc = plan.warps_per_cta;
     const int grid = (int)std::min<uint64_t>((nq + wpc - 1) / wpc,
                                              (uint64_t)plan.blocks_per_sm * h->sm_count);
+    int rc = ev_slices((uint64_t)grid * wpc);
+    if (rc) return rc;
+    qc.ev_scratch = qa.ev_scratch;
     if (hglob) {
       const uint64_t words = (uint64_t)grid * wpc * lc.hash_words;
       if (words > h->qhash_words) {

@@ -52,7 +52,10 @@ WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, ui
       w.vis_id = off; off += r16(4ull * vcap);
       w.vis_d = off; off += r16(4ull * vcap);
     }
-    w.ws = off; off += r16(4ull * vcap);  // evicted list
+    w.ws = off; off += 128;  // filter of the evicted ids
+    if (keep_vis) {          // the debug search keeps its evicted list here too
+      w.ev = off; off += r16(4ull * vcap);
+    }
     w.hash_global = hash_global ? 1u : 0u;
     w.hash_words = hash_bytes / 4;
     if (!hash_global) off += hash_bytes;
@@ -74,14 +77,18 @@ __device__ __forceinline__ SearchSmem carve_build(uint8_t* base, const WarpLayou
   S.vis_id = vis_g;
   S.vis_d = (float*)(vis_g + w.vcap);
   S.ev_id = nullptr;
+  S.ev_bloom = nullptr;
   S.hash = (uint32_t*)(base + w.ws);
   S.h24 = (int)w.h24;
   return S;
 }
 
 // query / debug layout: everything in shared memory
+// global_hash / global_ev: this warp's global slices (hash_global layouts; the
+// evicted list of layouts without keep_vis)
 __device__ __forceinline__ SearchSmem carve_query(uint8_t* base, const WarpLayout& w,
-                                                  uint32_t* global_hash = nullptr) {
+                                                  uint32_t* global_hash = nullptr,
+                                                  uint32_t* global_ev = nullptr) {
   SearchSmem S;
   S.qv = base + w.qv;
   S.fr_id = (uint32_t*)(base + w.fr_id);
@@ -92,8 +99,10 @@ __device__ __forceinline__ SearchSmem carve_query(uint8_t* base, const WarpLayou
   S.s_d = (float*)(base + w.s_d);
   S.vis_id = w.keep_vis ? (uint32_t*)(base + w.vis_id) : nullptr;
   S.vis_d = w.keep_vis ? (float*)(base + w.vis_d) : nullptr;
-  S.ev_id = (uint32_t*)(base + w.ws);
-  S.hash = w.hash_global ? global_hash : (uint32_t*)(base + w.ws + r16(4ull * w.vcap));
+  S.ev_bloom = (uint32_t*)(base + w.ws);
+  S.ev_id = w.keep_vis ? (uint32_t*)(base + w.ev) : global_ev;
+  S.hash = w.hash_global ? global_hash
+                         : (uint32_t*)(base + w.ws + 128 + (w.keep_vis ? r16(4ull * w.vcap) : 0));
   S.h24 = (int)w.h24;
   return S;
 }
@@ -116,7 +125,7 @@ __global__ void __launch_bounds__(FASTF ? 352 : 512, FASTF ? 2 : 1)
   SearchParams P;
   P.points = ix.points; P.stride = ix.stride; P.graph = ix.graph; P.Rp = ix.Rp; P.n = ix.n;
   P.d = ix.d; P.start = ra.start; P.L = ra.L; P.k = 0; P.cut = 0.0; P.limit = ix.n;
-  P.degree_limit = ix.R; P.hbits = lay.hbits; P.vcap = lay.vcap; P.query_mode = 0;
+  P.degree_limit = ix.R; P.hbits = lay.hbits; P.vcap = lay.vcap; P.ecap = 0; P.query_mode = 0;
   P.keep_visited = 1; P.err = ix.err;
   const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
   uint64_t cur = gw;
@@ -145,7 +154,8 @@ __global__ void __launch_bounds__(512) k_query(IndexView ix, QueryArgs qa, WarpL
   // large seen tables (beam widths above 128) live in this warp's global slice
   const SearchSmem S =
       carve_query((uint8_t*)smem_raw + (size_t)wic * lay.total, lay,
-                  lay.hash_global ? qa.hash_scratch + gw * (uint64_t)lay.hash_words : nullptr);
+                  lay.hash_global ? qa.hash_scratch + gw * (uint64_t)lay.hash_words : nullptr,
+                  qa.ev_scratch + gw * (uint64_t)qa.ev_cap);
   const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
   const uint64_t nitems = qa.cls_items ? (uint64_t)*qa.cls_count : qa.nq;
   uint64_t cur = gw;
@@ -161,8 +171,8 @@ __global__ void __launch_bounds__(512) k_query(IndexView ix, QueryArgs qa, WarpL
     }
     P.points = ix.points; P.stride = ix.stride; P.graph = ix.graph; P.Rp = ix.Rp; P.n = ix.n;
     P.d = ix.d; P.start = qa.start; P.L = Lq; P.k = qa.k; P.cut = qa.cut; P.limit = qa.limit;
-    P.degree_limit = qa.degree_limit; P.hbits = hash_bits_for(P.L); P.vcap = lay.vcap;
-    P.query_mode = 1; P.keep_visited = 0; P.err = ix.err;
+    P.degree_limit = qa.degree_limit; P.hbits = hash_bits_for(P.L); P.vcap = 0;
+    P.ecap = qa.ev_cap; P.query_mode = 1; P.keep_visited = 0; P.err = ix.err;
     load_vec(S.qv, qa.queries + q * qa.qstride, qb);
     __syncwarp();
     SearchOut o = warp_beam_search<DT, MT, FPL, CPL>(P, S, qa.skip_self ? q : (uint64_t)-1);
@@ -206,7 +216,7 @@ __global__ void __launch_bounds__(32) k_beam(IndexView ix, BeamArgs ba, WarpLayo
     SearchParams P;
     P.points = ix.points; P.stride = ix.stride; P.graph = ix.graph; P.Rp = ix.Rp; P.n = ix.n;
     P.d = ix.d; P.start = ba.start; P.L = ba.L; P.k = ba.k; P.cut = ba.cut; P.limit = ba.limit;
-    P.degree_limit = ba.degree_limit; P.hbits = lay.hbits; P.vcap = lay.vcap;
+    P.degree_limit = ba.degree_limit; P.hbits = lay.hbits; P.vcap = lay.vcap; P.ecap = lay.vcap;
     P.query_mode = ba.k > 0; P.keep_visited = 1; P.err = ix.err;
     load_vec(S.qv, ba.queries + q * ba.qstride, qb);
     __syncwarp();

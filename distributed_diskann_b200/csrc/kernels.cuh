@@ -22,6 +22,7 @@ struct WarpLayout {
   uint32_t fastf;     // build search with the fast form's seen filter (16-bit tags)
   uint32_t hash_global;  // query layout: the seen table lives in a global slice per warp
   uint32_t hash_words;   // its size in 32-bit words (16-byte multiple)
+  uint32_t ev;           // query layout: evicted list in shared memory (keep_vis layouts)
 };
 
 // Per-warp shared-memory carve-up of k_prune (byte offsets, 16-byte aligned).
@@ -142,6 +143,8 @@ struct QueryArgs {
   uint32_t* cls_queue;
   uint32_t Lvalid;         // largest valid beam width (the caller's Lmax; Lmax is the class's)
   uint32_t* hash_scratch;  // layouts with hash_global: one table per warp of the grid
+  uint32_t* ev_scratch;    // evicted lists, ev_cap ids per warp of the grid
+  uint32_t ev_cap;
 };
 
 // Beam-width classes of the bucketed query launch: class c serves beam widths

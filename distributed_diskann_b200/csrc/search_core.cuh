@@ -45,7 +45,8 @@ struct SearchSmem {
   float* s_d;
   uint32_t* vis_id;   // visited list in visit order (keep_visited), capacity vcap
   float* vis_d;
-  uint32_t* ev_id;    // visited ids pushed out of the frontier (query_mode), capacity vcap
+  uint32_t* ev_id;    // visited ids pushed out of the frontier (query_mode), capacity ecap
+  uint32_t* ev_bloom; // 1024-bit filter of the ids in ev_id (shared memory, query_mode)
   uint32_t* hash;     // 2^bits slots (shared memory): uint32 ids, or with h24
                       // a uint16 array of the low bits then a uint8 array of the high bits
   int h24;            // ids stored in 24 bits (every id < 0xFFFFFF); 0xFFFFFF = empty
@@ -120,7 +121,8 @@ struct SearchParams {
   uint64_t limit;
   uint32_t degree_limit;
   uint32_t hbits;
-  uint32_t vcap;
+  uint32_t vcap;        // visited-list capacity (keep_visited)
+  uint32_t ecap;        // evicted-list capacity (query_mode)
   int query_mode;       // track evicted visited entries for re-entry
   int keep_visited;     // record the visited list (build / debug)
   uint32_t* err;
@@ -131,6 +133,18 @@ struct SearchOut {
   uint32_t vis_n;       // number of visited nodes (= visited list length when kept)
   uint32_t cmps;        // distance computations (reference dist_cmps)
 };
+
+// The evicted list of a query search is scanned only for candidates whose id
+// may be in it: a 1024-bit filter of the evicted ids answers "maybe" or "no".
+__device__ __forceinline__ uint32_t ev_bloom_bit(uint32_t id) { return (id * 0x9E3779B1u) >> 22; }
+__device__ __forceinline__ void ev_bloom_add(uint32_t* bloom, uint32_t id) {
+  const uint32_t b = ev_bloom_bit(id);
+  atomicOr(&bloom[b >> 5], 1u << (b & 31));
+}
+__device__ __forceinline__ bool ev_bloom_maybe(const uint32_t* bloom, uint32_t id) {
+  const uint32_t b = ev_bloom_bit(id);
+  return (bloom[b >> 5] >> (b & 31)) & 1u;
+}
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m;
@@ -176,6 +190,7 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
     const uint32_t n16 =
         (FASTF ? fast_table_bytes(P.hbits) : hash_table_bytes(P.hbits, S.h24 != 0)) / 16u;
     for (uint32_t i = lane; i < n16; i += 32) h4[i] = none;
+    if (P.query_mode) S.ev_bloom[lane] = 0u;
   }
   if (lane == 0) {
     S.fr_id[0] = P.start;
@@ -409,7 +424,8 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
           a_ok[t] = true;
           if (P.query_mode) {
             uint32_t ev = 0;
-            for (uint32_t e = 0; e < ev_n; e++) ev += (S.ev_id[e] == ci) ? 1u : 0u;
+            if (ev_bloom_maybe(S.ev_bloom, ci))
+              for (uint32_t e = 0; e < ev_n; e++) ev += (S.ev_id[e] == ci) ? 1u : 0u;
             if (k < mf + ev) ci |= DD_VBIT;
           }
           a_id[t] = ci;
@@ -515,10 +531,14 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
         uint32_t eb = __ballot_sync(FULL, ev);
         if (ev) {
           uint32_t pos = ev_n + __popc(eb & lanemask_lt());
-          if (pos < P.vcap) S.ev_id[pos] = my_id[t] & ~DD_VBIT;
-          else dd_set_error(P.err, DD_EVIS_CAP);
+          if (pos < P.ecap) {
+            S.ev_id[pos] = my_id[t] & ~DD_VBIT;
+            ev_bloom_add(S.ev_bloom, my_id[t] & ~DD_VBIT);
+          } else {
+            dd_set_error(P.err, DD_EVIS_CAP);
+          }
         }
-        ev_n = min(P.vcap, ev_n + __popc(eb));
+        ev_n = min(P.ecap, ev_n + __popc(eb));
       }
     }
     fr_n = new_n;
@@ -544,10 +564,14 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
           uint32_t eb = __ballot_sync(FULL, ev);
           if (ev) {
             uint32_t pos = ev_n + __popc(eb & lanemask_lt());
-            if (pos < P.vcap) S.ev_id[pos] = S.fr_id[i] & ~DD_VBIT;
-            else dd_set_error(P.err, DD_EVIS_CAP);
+            if (pos < P.ecap) {
+              S.ev_id[pos] = S.fr_id[i] & ~DD_VBIT;
+              ev_bloom_add(S.ev_bloom, S.fr_id[i] & ~DD_VBIT);
+            } else {
+              dd_set_error(P.err, DD_EVIS_CAP);
+            }
           }
-          ev_n = min(P.vcap, ev_n + __popc(eb));
+          ev_n = min(P.ecap, ev_n + __popc(eb));
         }
       }
       fr_n = keep_n;
