@@ -38,6 +38,11 @@ sys.path.insert(0, ROOT)
 METRIC = "build pts/s; QPS@recall10>=0.95, BF16/INT8+rerank vs exact plain, 1 B200"
 
 
+def log(msg):
+    """Progress on stderr (the JSON line alone goes to stdout)."""
+    print(f"[bench] {msg}", file=sys.stderr, flush=True)
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -368,6 +373,7 @@ def main():
     clk = clocks.stop()
     t_max = max_over_ranks(t_dev)
     value = MR.whole_job_rate(world, n, args.steps, t_max)
+    log(f"fast build: {value:.4g} points/s, {1000 * t_max / args.steps:.1f} ms per build")
 
     # ---- e2e through the C ABI with host buffers
     barrier()
@@ -397,11 +403,14 @@ def main():
     t_plain = max_over_ranks(ev0.elapsed_time(ev1) / 1000.0)
     plain_value = MR.whole_job_rate(world, n, ksp, t_plain)
     plain_same = bool(np.array_equal(gi.graph(), graph_fast))
+    log(f"plain build: {plain_value:.4g} points/s, same graph as fast: {plain_same}")
     st_plain = gi.build(w.L, w.alpha, collect_stats=True, mode="plain")
 
     # ---- one instrumented build: statistics + per-kernel device times
     st = gi.build(w.L, w.alpha, collect_stats=True, mode="fast")
     g = gi.graph()
+    log(f"stats fast: {st}")
+    log(f"stats plain: {st_plain}")
     deg = g[:, 0]
     es = 4 if w.dtype == "f32" else 1
     dsz = w.d * es
@@ -464,7 +473,9 @@ def main():
                 t = timed_search(Ls, L)
                 rec = D.recall_with_ties(ids.cpu().numpy().astype(np.uint32), gt_i, gt_d, k)
                 sweep.append({"L": L, "qps": nq / t, "recall10": rec})
+                log(f"{form} L={L}: {nq / t:.4g} QPS, recall@10 {rec:.4f}")
             t = timed_search(Lmix, max(w.sweep_L))
+            log(f"{form} mixed L: {nq / t:.4g} QPS")
             ok = [s for s in sweep if s["recall10"] >= 0.95]
             qres[form] = {"sweep": sweep, "mixed_L_qps": nq / t,
                           "qps_at_recall10_0.95": max(s["qps"] for s in ok) if ok else None}
