@@ -201,22 +201,23 @@ struct ElemSize { static constexpr int v = (DT == DD_F32) ? 4 : 1; };
 // reference's value).  Float data must keep the reference's summation order:
 // G must be 1 and the lane runs Dist::eval.  Every lane of the warp must call
 // it (the group reduction shuffles); lanes with act == false return 0.
-template <int DT, int MT>
+// NB: 16-byte words a lane loads per batch (its registers in flight).
+template <int DT, int MT, int NB = 8>
 __device__ __forceinline__ float dist_group(const uint4* q, const uint8_t* row, uint32_t d,
                                             uint32_t sub, uint32_t G, bool act) {
   if (DT == DD_F32) return act ? Dist<DT, MT>::eval(q, row, d) : 0.f;
   const uint32_t nv = (d + 15) >> 4;
   const uint4* r4 = (const uint4*)row;
   uint32_t acc = 0;
-  for (uint32_t w0 = sub; w0 < nv; w0 += 8 * G) {
-    uint4 y[8];
+  for (uint32_t w0 = sub; w0 < nv; w0 += NB * G) {
+    uint4 y[NB];
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
+    for (int i = 0; i < NB; i++) {
       const uint32_t w = w0 + (uint32_t)i * G;
       y[i] = (act && w < nv) ? __ldg(r4 + w) : make_uint4(0, 0, 0, 0);
     }
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
+    for (int i = 0; i < NB; i++) {
       const uint32_t w = w0 + (uint32_t)i * G;
       if (w < nv) {
         const uint4 x = q[w];

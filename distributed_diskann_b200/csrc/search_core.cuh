@@ -354,8 +354,8 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
         const uint32_t k = k0 + (lane >> lg);
         const bool act = k < nk;
         const uint32_t id = act ? S.s_id[k] : 0u;
-        const float dist = dist_group<DT, MT>((const uint4*)S.qv, P.points + (uint64_t)id * P.stride,
-                                              P.d, sub, G, act);
+        const float dist = dist_group<DT, MT, FASTF ? 4 : 8>(
+            (const uint4*)S.qv, P.points + (uint64_t)id * P.stride, P.d, sub, G, act);
         const bool pass = act && sub == 0 && dist < cutoff;
         const uint32_t pb = __ballot_sync(FULL, pass);
         if (pass) {
@@ -383,7 +383,8 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
       for (uint32_t j = 0; j < nc; j++) {
         float dj = S.c_d[j];
         uint32_t ij = S.c_id[j];
-        r += (pair_less(dj, ij, di, ii) || (dj == di && ij == ii && j < i)) ? 1u : 0u;
+        // (the fast form's rows hold no repeated id, so no identical copies)
+        r += (pair_less(dj, ij, di, ii) || (!FASTF && dj == di && ij == ii && j < i)) ? 1u : 0u;
       }
       S.s_id[r] = ii;
       S.s_d[r] = di;
@@ -472,6 +473,20 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
     scan0 = min(ub0, nxt_pos >= 0 ? (uint32_t)nxt_pos : new_n);
     uint32_t my_id[FPL], my_pos[FPL];
     float my_d[FPL];
+    // Fast form with few kept candidates (the common case once the frontier
+    // is full): every entry's shift is counted from the broadcast ub_j, with
+    // no per-entry binary search.
+    const bool count_shift = FASTF && nkeep <= 8;
+    uint32_t shift[FPL];
+#pragma unroll
+    for (int t = 0; t < FPL; t++) shift[t] = 0;
+    if (count_shift) {
+      for (uint32_t j = 0; j < nkeep; j++) {
+        const uint32_t ubj = S.s_id[j];
+#pragma unroll
+        for (int t = 0; t < FPL; t++) shift[t] += (ubj <= lane + 32u * t) ? 1u : 0u;
+      }
+    }
 #pragma unroll
     for (int t = 0; t < FPL; t++) {
       uint32_t i = lane + 32 * t;
@@ -482,11 +497,15 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
         if (i < ub0) {
           my_pos[t] = i;  // unmoved: not rewritten
         } else {
-          uint32_t lo = 1, hi = nkeep;
-          while (lo < hi) {
-            uint32_t mid = (lo + hi) >> 1;
-            if (S.s_id[mid] <= i) lo = mid + 1;
-            else hi = mid;
+          uint32_t lo = shift[t];
+          if (!count_shift) {
+            uint32_t hi = nkeep;
+            lo = 1;
+            while (lo < hi) {
+              uint32_t mid = (lo + hi) >> 1;
+              if (S.s_id[mid] <= i) lo = mid + 1;
+              else hi = mid;
+            }
           }
           my_id[t] = S.fr_id[i];
           my_d[t] = S.fr_d[i];
