@@ -36,6 +36,7 @@ struct dd_index {
   // build scratch (grown on demand, kept for reuse)
   uint64_t bcap = 0;        // batch capacity of the scratch below
   uint32_t* new_out = nullptr;
+  float* new_key = nullptr;  // distances of new_out's entries (fast form)
   uint32_t* stat_vis = nullptr;
   uint32_t* stat_cmps = nullptr;
   uint32_t* sort_t[2] = {nullptr, nullptr};  // semisort ping-pong buffers
@@ -180,12 +181,13 @@ int ensure_build_scratch(dd_index* h, uint64_t B) {
   }
   if (B <= h->bcap) return DD_OK;
   h->scratch_gen++;
-  void* old[] = {h->new_out, h->stat_vis, h->stat_cmps, h->sort_t[0], h->sort_t[1], h->sort_v[0],
+  void* old[] = {h->new_out, h->new_key, h->stat_vis, h->stat_cmps, h->sort_t[0], h->sort_t[1], h->sort_v[0],
                  h->sort_v[1], h->hist, h->heads, h->flags, h->big, h->gcand, h->gkey,
                  h->gpos, h->gbits, h->granges};
   for (void* p : old) dfree(p);
   const uint64_t E = B * h->Rp;
   CK(dalloc(&h->new_out, E));
+  CK(dalloc(&h->new_key, E));
   CK(dalloc(&h->stat_vis, B));
   CK(dalloc(&h->stat_cmps, B));
   for (int i = 0; i < 2; i++) {
@@ -463,6 +465,7 @@ int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& r
     ra.alpha = alpha;
     ra.start = P->start_point;
     ra.new_out = h->new_out;
+    ra.new_key = bp.fast ? h->new_key : nullptr;
     ra.stat_vis = h->stat_vis;
     ra.stat_cmps = h->stat_cmps;
     ra.vis_all = h->vis_all;
@@ -584,7 +587,7 @@ int dd_create(int dtype, int metric, uint64_t n, uint32_t d, uint32_t R, int dev
 int dd_destroy(dd_index* h) {
   if (!h) return DD_OK;
   cudaSetDevice(h->device);
-  void* ptrs[] = {h->points, h->graph, h->err, h->new_out, h->stat_vis, h->stat_cmps,
+  void* ptrs[] = {h->points, h->graph, h->err, h->new_out, h->new_key, h->stat_vis, h->stat_cmps,
                   h->sort_t[0], h->sort_t[1], h->sort_v[0], h->sort_v[1], h->hist, h->heads,
                   h->flags, h->counters, h->big, h->block_sums, h->acc, h->gcand, h->gkey,
                   h->gpos, h->gbits, h->granges, h->vis_all, h->ref_rows};
@@ -990,6 +993,7 @@ RoundArgs shard_round_args(dd_index* h, uint64_t floor, uint64_t B, uint32_t* ro
   ra.alpha = h->shard_params.alpha;
   ra.start = h->shard_params.start_point;
   ra.new_out = rows;
+  ra.new_key = nullptr;  // the exchanged rows carry no distances: the reverse step recomputes
   ra.stat_vis = h->stat_vis;
   ra.stat_cmps = h->stat_cmps;
   ra.vis_all = h->vis_all;

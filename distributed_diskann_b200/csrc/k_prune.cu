@@ -82,7 +82,8 @@ __global__ void __launch_bounds__(512) k_prune(IndexView ix, RoundArgs ra, Prune
     __syncwarp();
     warp_std_sort(Pm, m);
     warp_greedy_select_fast<DT, MT, true, TC>(ix.points, ix.stride, ix.d, p, Pm, m, ra.alpha, ix.R,
-                                    ra.new_out + b * ix.Rp, ix.Rp, Pm.sel);
+                                    ra.new_out + b * ix.Rp, ix.Rp, Pm.sel,
+                                    ra.new_key ? ra.new_key + b * ix.Rp : nullptr);
   }
 }
 

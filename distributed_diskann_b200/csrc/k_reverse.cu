@@ -69,10 +69,14 @@ __device__ void reverse_one(const IndexView& ix, const RoundArgs& ra, const Reve
   const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
   load_vec(tv, ix.points + (uint64_t)t * ix.stride, qb);
   __syncwarp();
+  // a source's distance to t is the one its own prune selected t with (the
+  // distances are symmetric bit for bit: (a-b)^2 = (b-a)^2, a*b = b*a, same
+  // summation order), when the insert prune kept it
   for (uint32_t j = lane; j < s; j += 32) {
     uint32_t c = (uint32_t)(ra.floor + sk[j] / ix.Rp);
     Pm.cid[j] = c;
-    Pm.ckey[j] = Dist<DT, MT>::eval(tv, ix.points + (uint64_t)c * ix.stride, ix.d);
+    Pm.ckey[j] = ra.new_key ? ra.new_key[sk[j]]
+                            : Dist<DT, MT>::eval(tv, ix.points + (uint64_t)c * ix.stride, ix.d);
   }
   for (uint32_t j = lane; j < deg; j += 32) {
     uint32_t c = row[j];
@@ -179,9 +183,11 @@ __global__ void __launch_bounds__(kBigThreads) k_reverse_big(IndexView ix, Round
       continue;
     }
     for (uint32_t j = tid; j < s; j += blockDim.x) {
-      uint32_t c = (uint32_t)(ra.floor + rs.sv[start + j] / ix.Rp);
+      const uint32_t key = rs.sv[start + j];
+      uint32_t c = (uint32_t)(ra.floor + key / ix.Rp);
       cid[j] = c;
-      ckey[j] = Dist<DT, MT>::eval(tv, ix.points + (uint64_t)c * ix.stride, ix.d);
+      ckey[j] = ra.new_key ? ra.new_key[key]
+                           : Dist<DT, MT>::eval(tv, ix.points + (uint64_t)c * ix.stride, ix.d);
     }
     for (uint32_t j = tid; j < deg; j += blockDim.x) {
       uint32_t c = row[j];

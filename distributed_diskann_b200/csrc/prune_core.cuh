@@ -301,17 +301,22 @@ __device__ __forceinline__ int cta_partition_rank(const ddsort::Arr<uint32_t>& A
 
 // Greedy selection over the sorted candidates; writes the selected ids to
 // out_row[0, nsel) and DD_NONE to out_row[nsel, Rp).  Returns nsel.
+// out_key (may be null): the selected entries' distances to p, beside out_row.
 template <int DT, int MT>
 __device__ uint32_t warp_greedy_select(const uint8_t* points, uint64_t stride, uint32_t d,
                                        uint32_t p, const PruneSmem& S, uint32_t m, double alpha,
-                                       uint32_t R, uint32_t* out_row, uint32_t Rp) {
+                                       uint32_t R, uint32_t* out_row, uint32_t Rp,
+                                       float* out_key = nullptr) {
   const uint32_t lane = lane_id();
   uint32_t nsel = 0, idx = 0;
   while (nsel < R && idx < m) {
     const uint32_t ps = S.cid[idx];
     idx++;
     if (ps == p || ps == DD_NONE) continue;
-    if (lane == 0) out_row[nsel] = ps;
+    if (lane == 0) {
+      out_row[nsel] = ps;
+      if (out_key) out_key[nsel] = S.ckey[idx - 1];
+    }
     nsel++;
     const uint8_t* prow = points + (uint64_t)ps * stride;
     for (uint32_t i = idx + lane; i < m; i += 32) {
@@ -424,7 +429,7 @@ template <int DT, int MT>
 __device__ uint32_t warp_greedy_select_reg(const uint8_t* points, uint64_t stride, uint32_t d,
                                            uint32_t p, const PruneSmem& S, uint32_t m,
                                            double alpha, uint32_t R, uint32_t* out_row,
-                                           uint32_t Rp, uint4* sel) {
+                                           uint32_t Rp, uint4* sel, float* out_key = nullptr) {
   constexpr int NVM = RegRow<DT>::NVM;
   const uint32_t FULL = 0xffffffffu;
   const uint32_t lane = lane_id();
@@ -457,6 +462,7 @@ __device__ uint32_t warp_greedy_select_reg(const uint8_t* points, uint64_t strid
       uint4* dst = sel + (uint64_t)nsel * nv;
       if (lane == i) {
         out_row[nsel] = cj;
+        if (out_key) out_key[nsel] = S.ckey[j];
 #pragma unroll
         for (int k = 0; k < NVM; k++)
           if ((uint32_t)k < nv) dst[k] = row[k];
@@ -613,7 +619,7 @@ template <int DT, int MT, bool PREFETCH = true>
 __device__ uint32_t warp_greedy_select_mma(const uint8_t* points, uint64_t stride, uint32_t d,
                                            uint32_t p, const PruneSmem& S, uint32_t m,
                                            double alpha, uint32_t R, uint32_t* out_row,
-                                           uint32_t Rp, uint4* sel) {
+                                           uint32_t Rp, uint4* sel, float* out_key = nullptr) {
   const uint32_t FULL = 0xffffffffu;
   const uint32_t lane = lane_id(), g = lane >> 2, t = lane & 3;
   uint32_t* rw = (uint32_t*)sel;
@@ -729,7 +735,10 @@ __device__ uint32_t warp_greedy_select_mma(const uint8_t* points, uint64_t strid
       const uint32_t j = lane >> 1, h = lane & 1;
       const bool s = (selm >> j) & 1u;
       const uint32_t k = __popc(selm & ((1u << j) - 1u));
-      if (s && h == 0) out_row[nsel + k] = S.cid[c0 + j];
+      if (s && h == 0) {
+        out_row[nsel + k] = S.cid[c0 + j];
+        if (out_key) out_key[nsel + k] = S.ckey[c0 + j];
+      }
       uint4 v[4];
       int nrm = 0;
       if (s) {
@@ -763,14 +772,15 @@ __device__ __forceinline__ uint32_t warp_greedy_select_fast(const uint8_t* point
                                                             const PruneSmem& S, uint32_t m,
                                                             double alpha, uint32_t R,
                                                             uint32_t* out_row, uint32_t Rp,
-                                                            uint4* sel) {
+                                                            uint4* sel, float* out_key = nullptr) {
   if (TENSOR && DT != DD_F32 && greedy_uses_mma(d, DT))
     return warp_greedy_select_mma<DT, MT, PREFETCH>(points, stride, d, p, S, m, alpha, R,
-                                                    out_row, Rp, sel);
+                                                    out_row, Rp, sel, out_key);
   if (row_words16(d, DT) <= (uint32_t)RegRow<DT>::NVM) {
-    return warp_greedy_select_reg<DT, MT>(points, stride, d, p, S, m, alpha, R, out_row, Rp, sel);
+    return warp_greedy_select_reg<DT, MT>(points, stride, d, p, S, m, alpha, R, out_row, Rp, sel,
+                                          out_key);
   }
-  return warp_greedy_select<DT, MT>(points, stride, d, p, S, m, alpha, R, out_row, Rp);
+  return warp_greedy_select<DT, MT>(points, stride, d, p, S, m, alpha, R, out_row, Rp, out_key);
 }
 
 // byte offset of the (16-byte aligned) selected-row area inside a prune
