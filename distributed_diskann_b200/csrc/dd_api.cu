@@ -235,6 +235,22 @@ int ensure_vis_all(dd_index* h, uint64_t words) {
   return DD_OK;
 }
 
+// Graph rows never hold an id twice during the build: the fast form's seen
+// filter relies on it (search_core.cuh).  Reverse edges are appended without
+// a membership check (include/utils/graph.h:84-93), so a row gets a repeat when
+// the source is already in it: in the second pass of a two-pass build, and
+// when the start point is inserted after points that linked to it (their
+// searches start there), because its own reverse edges then reach rows that
+// already name it.  A start point inserted first (point 0, the identity
+// order's first) or never inserted (beyond max_build) cannot be in a row
+// before its own insertion round.
+bool rows_without_repeats(const dd_index* h, const dd_build_params* P) {
+  if (P->two_pass) return false;
+  const uint64_t m = (P->max_build && !P->knn_mode) ? std::min<uint64_t>(P->max_build, h->n) : h->n;
+  const uint64_t start = P->knn_mode ? 0 : P->start_point;
+  return start == 0 || start >= m;
+}
+
 // room for `words` work-queue counters
 int ensure_queues(dd_index* h, uint64_t words) {
   if (words <= h->queue_words) return DD_OK;
@@ -801,9 +817,7 @@ int build_once(dd_index* h, const dd_build_params* P, uint32_t vcap, dd_stats* s
   if (rc) return rc;
   BuildPlan bp;
   bp.fast = P->mode == DD_MODE_FAST;
-  // the fast form's seen filter needs ids below 2^24 and rows without repeats
-  // (single-pass builds); two-pass builds replay the reference's filter
-  const bool fastf = bp.fast && use_h24(h) && !P->two_pass;
+  const bool fastf = bp.fast && use_h24(h) && rows_without_repeats(h, P);
   bp.slay = make_search_layout(h->d, h->dtype, P->L, h->Rp, vcap, true, use_h24(h), true, fastf);
   if (bp.slay.total > 227 * 1024)
     return fail(h, DD_ERR_UNSUPPORTED, "per-warp shared memory %u B too large (L=%u)",
@@ -976,7 +990,7 @@ BuildPlan shard_plan(dd_index* h) {
   const uint32_t vcap = P->vcap ? P->vcap : 8 * P->L;
   BuildPlan bp;
   bp.fast = P->mode == DD_MODE_FAST;
-  const bool fastf = bp.fast && use_h24(h);
+  const bool fastf = bp.fast && use_h24(h) && rows_without_repeats(h, P);
   bp.slay = make_search_layout(h->d, h->dtype, P->L, h->Rp, vcap, true, use_h24(h), true, fastf);
   bp.play = make_prune_layout(h->d, h->dtype, h->Rp, bp.slay.ccap, bp.fast);
   bp.splan = plan_search(view(h), bp.slay, P->L);

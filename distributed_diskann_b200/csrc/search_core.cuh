@@ -58,12 +58,12 @@ __host__ __device__ inline uint32_t hash_table_bytes(uint32_t hbits, bool h24) {
 }
 
 // ---------------------------------------------------------------------------
-// The fast form's "seen" filter (build searches of single-pass builds with
-// every id below 2^24 - 1).  In a build search (k = 0, no k-cut) the filter
+// The fast form's "seen" filter (build searches of builds whose graph rows
+// never hold an id twice, with every id below 2^24 - 1; the host decides,
+// rows_without_repeats).  In a build search (k = 0, no k-cut) the filter
 // only decides which neighbours get their distance computed: an id it lets
 // through twice is re-evaluated, fails the cutoff or is already in the
-// frontier, and set_union drops the copy (graph rows of a single-pass build
-// hold no repeated id).  So any filter without false positives gives the
+// frontier, and set_union drops the copy.  So any filter without false positives gives the
 // reference's frontier, visited list and graph; only the dist_cmps count
 // moves.  This one keeps 2^hbits slots like the reference's, but hashes ids
 // with a bijection of [0, 2^24) and stores the 24 - hbits quotient bits in a
