@@ -219,35 +219,6 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
       a_pre[t] = (j < dl) ? __ldg(prow + j) : DD_NONE;
     }
   };
-  // Fast form: the row of the next unvisited frontier entry is loaded at the
-  // start of each step.  When that entry is also the node expected next, its
-  // row is ready at the end of the step: it becomes the next step's row, and
-  // the vectors of the neighbours the seen table would keep are brought into
-  // L2 a step ahead of their distance computations.
-  uint32_t bpred = DD_NONE;
-  uint32_t b_pre[CPL];
-  const uint32_t vbytes = P.d * (uint32_t)ElemSize<DT>::v;
-  auto advance_to = [&](uint32_t node) {
-    if (FASTF && node == bpred) {
-      pred = node;
-      const uint16_t* tab = (const uint16_t*)S.hash;
-#pragma unroll
-      for (int t = 0; t < CPL; t++) {
-        const uint32_t at = b_pre[t];
-        a_pre[t] = at;
-        if (at != DD_NONE && at < P.n && (uint64_t)at != self_id) {
-          const uint32_t f = mix24(at);
-          if (tab[f & hmask] != (uint16_t)(f >> P.hbits)) {
-            const uint8_t* v = P.points + (uint64_t)at * P.stride;
-            for (uint32_t off = 0; off < vbytes; off += 128)
-              asm volatile("prefetch.global.L2 [%0];" ::"l"(v + off));
-          }
-        }
-      }
-    } else {
-      prefetch_row(node);
-    }
-  };
 
   while (num_visited < P.limit) {
     // ---- closest unvisited frontier entry (every entry before scan0 is visited)
@@ -298,20 +269,8 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
       if (b) { nxt_pos = (int)(base + __ffs(b) - 1); break; }
     }
     // its row is brought into L2 now (128-byte lines, one per lane); the
-    // speculative load of the next row then usually hits L2.  The fast form
-    // loads it into registers instead (see advance_to).
-    if (FASTF) {
-      bpred = DD_NONE;
-      if (nxt_pos >= 0) {
-        bpred = S.fr_id[nxt_pos];
-        const uint32_t* nrow = P.graph + (uint64_t)bpred * P.Rp;
-#pragma unroll
-        for (int t = 0; t < CPL; t++) {
-          const uint32_t j = 32 * t + lane;
-          b_pre[t] = (j < dl) ? __ldg(nrow + j) : DD_NONE;
-        }
-      }
-    } else if (nxt_pos >= 0 && lane * 32u < dl) {
+    // speculative load of the next row then usually hits L2
+    if (nxt_pos >= 0 && lane * 32u < dl) {
       const uint32_t* nrow = P.graph + (uint64_t)S.fr_id[nxt_pos] * P.Rp + lane * 32u;
       asm volatile("prefetch.global.L2 [%0];" ::"l"(nrow));
     }
@@ -409,7 +368,7 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
     }
     __syncwarp();
     if (nc == 0) {
-      if (nxt_pos >= 0) advance_to(S.fr_id[nxt_pos]);
+      if (nxt_pos >= 0) prefetch_row(S.fr_id[nxt_pos]);
       scan0 = nxt_pos >= 0 ? (uint32_t)nxt_pos : fr_n;
       continue;
     }
@@ -498,7 +457,7 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
       if (nxt_pos >= 0 &&
           (nid == DD_NONE || !pair_less(S.c_d[0], nid, S.fr_d[nxt_pos], S.fr_id[nxt_pos])))
         nid = S.fr_id[nxt_pos];
-      if (nid != DD_NONE) advance_to(nid);
+      if (nid != DD_NONE) prefetch_row(nid);
     }
     if (nkeep == 0) {
       scan0 = nxt_pos >= 0 ? (uint32_t)nxt_pos : fr_n;
