@@ -576,9 +576,10 @@ __device__ __forceinline__ void mma_tile_16x16(const uint32_t* rw, uint32_t ra0,
 // "d <= occlusion_threshold".  The result is clamped to +-2^25, which keeps
 // that equivalence for every |d| < 2^24; floor(key / alpha) is off by at most
 // one, so two correction steps each way suffice.
-__device__ __forceinline__ int occlusion_threshold(double alpha, float key) {
+// inv_alpha = 1 / alpha (the estimate may be off by one; the steps fix it).
+__device__ __forceinline__ int occlusion_threshold(double alpha, double inv_alpha, float key) {
   const double k = (double)key, lim = 33554432.0;
-  double x = floor(k / alpha);
+  double x = floor(k * inv_alpha);
   x = fmin(fmax(x, -lim), lim);
   for (int it = 0; it < 2 && x < lim && __dmul_rn(alpha, x + 1.0) <= k; it++) x += 1.0;
   for (int it = 0; it < 2 && x > -lim && __dmul_rn(alpha, x) > k; it++) x -= 1.0;
@@ -627,6 +628,7 @@ __device__ uint32_t warp_greedy_select_mma(const uint8_t* points, uint64_t strid
   int* cthr = norms + Rp + kMmaChunk;
   const uint32_t qb = (d + 15u) & ~15u;   // padded row bytes (integer data)
   const uint32_t KS = (qb + 31u) >> 5;    // k-steps of 32 bytes
+  const double inv_alpha = 1.0 / alpha;
   const uint32_t NW = 2u * KS;            // 16-byte words staged per row
   // A chunk's rows are loaded into registers (two lanes per member, 16-byte
   // words h, h+2, h+4, h+6): with PREFETCH one chunk ahead of its tiles.
@@ -675,7 +677,7 @@ __device__ uint32_t warp_greedy_select_mma(const uint8_t* points, uint64_t strid
       if (h == 0) {
         norms[r] = (int)nrm;
         // occlusion of member j: L2 |a|^2 - 2 a.b <= T_j - |b|^2, MIPS -a.b <= T_j
-        const int T = alive ? occlusion_threshold(alpha, S.ckey[c0 + j]) : 0;
+        const int T = alive ? occlusion_threshold(alpha, inv_alpha, S.ckey[c0 + j]) : 0;
         cthr[j] = MT == DD_L2 ? T - (int)nrm : T;
       }
       const bool a2 = __shfl_sync(FULL, alive ? 1 : 0, (2u * lane) & 31u) != 0;
@@ -801,6 +803,81 @@ __host__ __device__ inline uint32_t prune_ws_bytes_sel(uint32_t cap, uint32_t se
 // In-place ascending sort of (key, id) pairs by (key, id) on one warp:
 // bitonic network with all comparators ascending (the partner of i in the
 // first step of each stage is i ^ (k - 1)), so a ragged tail needs no padding.
+// The same order for n <= 32 R with the elements in registers: element
+// i = lane + 32 r is register r of a lane; partners 32 apart or more are in the
+// same lane, closer ones are exchanged with shuffles.  Padding sorts last.
+template <int R>
+__device__ __forceinline__ void warp_sort_pairs_reg(uint32_t* ids, float* keys, uint32_t n) {
+  const uint32_t lane = lane_id();
+  float k[R];
+  uint32_t v[R];
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const uint32_t i = lane + 32u * r;
+    k[r] = i < n ? keys[i] : INFINITY;
+    v[r] = i < n ? ids[i] : DD_NONE;
+  }
+  constexpr uint32_t N = 32u * R;
+#pragma unroll
+  for (uint32_t sz = 2; sz <= N; sz <<= 1) {
+#pragma unroll
+    for (uint32_t j = sz >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+        const uint32_t jr = j >> 5;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          if ((r & jr) == 0) {
+            const int r2 = r | (int)jr;
+            const bool asc = ((lane + 32u * r) & sz) == 0;
+            const bool sw = asc ? pair_less(k[r2], v[r2], k[r], v[r])
+                                : pair_less(k[r], v[r], k[r2], v[r2]);
+            if (sw) {
+              const float tk = k[r]; k[r] = k[r2]; k[r2] = tk;
+              const uint32_t tv = v[r]; v[r] = v[r2]; v[r2] = tv;
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          const float ok = __shfl_xor_sync(0xffffffffu, k[r], j);
+          const uint32_t ov = __shfl_xor_sync(0xffffffffu, v[r], j);
+          const bool asc = ((lane + 32u * r) & sz) == 0;
+          const bool lower = (lane & j) == 0;
+          const bool take = (lower == asc) ? pair_less(ok, ov, k[r], v[r])
+                                           : pair_less(k[r], v[r], ok, ov);
+          if (take) {
+            k[r] = ok;
+            v[r] = ov;
+          }
+        }
+      }
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const uint32_t i = lane + 32u * r;
+    if (i < n) {
+      keys[i] = k[r];
+      ids[i] = v[r];
+    }
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void warp_sort_pairs(uint32_t* ids, float* keys, uint32_t n);
+
+// Sorts (keys, ids)[0, n) by (key, id): registers up to 256 elements, the
+// shared-memory network beyond.
+__device__ __forceinline__ void warp_sort_pairs_any(uint32_t* ids, float* keys, uint32_t n) {
+  if (n <= 32) warp_sort_pairs_reg<1>(ids, keys, n);
+  else if (n <= 64) warp_sort_pairs_reg<2>(ids, keys, n);
+  else if (n <= 128) warp_sort_pairs_reg<4>(ids, keys, n);
+  else if (n <= 256) warp_sort_pairs_reg<8>(ids, keys, n);
+  else warp_sort_pairs(ids, keys, n);
+}
+
 __device__ __forceinline__ void warp_sort_pairs(uint32_t* ids, float* keys, uint32_t n) {
   const uint32_t lane = lane_id();
   uint32_t N = 1;
