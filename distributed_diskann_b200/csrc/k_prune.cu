@@ -64,8 +64,7 @@ __global__ void __launch_bounds__(512) k_prune(IndexView ix, RoundArgs ra, Prune
       Pm.ckey[j] = __uint_as_float(vis[vcap + j]);
     }
     __syncwarp();
-    if (TC) warp_sort_pairs_any(Pm.cid, Pm.ckey, m);  // the fast form sorts in registers
-    else warp_sort_pairs(Pm.cid, Pm.ckey, m);
+    warp_sort_pairs(Pm.cid, Pm.ckey, m);
     // robustPrune adds p's current out-list (round-start snapshot)
     const uint32_t* prow = ix.graph + (uint64_t)p * ix.Rp;
     for (uint32_t b0 = 0; b0 < ix.Rp; b0 += 32) {

@@ -803,81 +803,6 @@ __host__ __device__ inline uint32_t prune_ws_bytes_sel(uint32_t cap, uint32_t se
 // In-place ascending sort of (key, id) pairs by (key, id) on one warp:
 // bitonic network with all comparators ascending (the partner of i in the
 // first step of each stage is i ^ (k - 1)), so a ragged tail needs no padding.
-// The same order for n <= 32 R with the elements in registers: element
-// i = lane + 32 r is register r of a lane; partners 32 apart or more are in the
-// same lane, closer ones are exchanged with shuffles.  Padding sorts last.
-template <int R>
-__device__ __forceinline__ void warp_sort_pairs_reg(uint32_t* ids, float* keys, uint32_t n) {
-  const uint32_t lane = lane_id();
-  float k[R];
-  uint32_t v[R];
-#pragma unroll
-  for (int r = 0; r < R; r++) {
-    const uint32_t i = lane + 32u * r;
-    k[r] = i < n ? keys[i] : INFINITY;
-    v[r] = i < n ? ids[i] : DD_NONE;
-  }
-  constexpr uint32_t N = 32u * R;
-#pragma unroll
-  for (uint32_t sz = 2; sz <= N; sz <<= 1) {
-#pragma unroll
-    for (uint32_t j = sz >> 1; j > 0; j >>= 1) {
-      if (j >= 32) {
-        const uint32_t jr = j >> 5;
-#pragma unroll
-        for (int r = 0; r < R; r++) {
-          if ((r & jr) == 0) {
-            const int r2 = r | (int)jr;
-            const bool asc = ((lane + 32u * r) & sz) == 0;
-            const bool sw = asc ? pair_less(k[r2], v[r2], k[r], v[r])
-                                : pair_less(k[r], v[r], k[r2], v[r2]);
-            if (sw) {
-              const float tk = k[r]; k[r] = k[r2]; k[r2] = tk;
-              const uint32_t tv = v[r]; v[r] = v[r2]; v[r2] = tv;
-            }
-          }
-        }
-      } else {
-#pragma unroll
-        for (int r = 0; r < R; r++) {
-          const float ok = __shfl_xor_sync(0xffffffffu, k[r], j);
-          const uint32_t ov = __shfl_xor_sync(0xffffffffu, v[r], j);
-          const bool asc = ((lane + 32u * r) & sz) == 0;
-          const bool lower = (lane & j) == 0;
-          const bool take = (lower == asc) ? pair_less(ok, ov, k[r], v[r])
-                                           : pair_less(k[r], v[r], ok, ov);
-          if (take) {
-            k[r] = ok;
-            v[r] = ov;
-          }
-        }
-      }
-    }
-  }
-  __syncwarp();
-#pragma unroll
-  for (int r = 0; r < R; r++) {
-    const uint32_t i = lane + 32u * r;
-    if (i < n) {
-      keys[i] = k[r];
-      ids[i] = v[r];
-    }
-  }
-  __syncwarp();
-}
-
-__device__ __forceinline__ void warp_sort_pairs(uint32_t* ids, float* keys, uint32_t n);
-
-// Sorts (keys, ids)[0, n) by (key, id): registers up to 256 elements, the
-// shared-memory network beyond.
-__device__ __forceinline__ void warp_sort_pairs_any(uint32_t* ids, float* keys, uint32_t n) {
-  if (n <= 32) warp_sort_pairs_reg<1>(ids, keys, n);
-  else if (n <= 64) warp_sort_pairs_reg<2>(ids, keys, n);
-  else if (n <= 128) warp_sort_pairs_reg<4>(ids, keys, n);
-  else if (n <= 256) warp_sort_pairs_reg<8>(ids, keys, n);
-  else warp_sort_pairs(ids, keys, n);
-}
-
 __device__ __forceinline__ void warp_sort_pairs(uint32_t* ids, float* keys, uint32_t n) {
   const uint32_t lane = lane_id();
   uint32_t N = 1;
