@@ -485,6 +485,7 @@ int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& r
     ra.stat_vis = h->stat_vis;
     ra.stat_cmps = h->stat_cmps;
     ra.vis_all = h->vis_all;
+    ra.vis_sorted_tail = bp.slay.fastf ? 1 : 0;
     ra.qsearch = nullptr;
     ra.qprune = nullptr;
     if (tune && B >= kTuneItems) {
@@ -1011,6 +1012,7 @@ RoundArgs shard_round_args(dd_index* h, uint64_t floor, uint64_t B, uint32_t* ro
   ra.stat_vis = h->stat_vis;
   ra.stat_cmps = h->stat_cmps;
   ra.vis_all = h->vis_all;
+  ra.vis_sorted_tail = shard_plan(h).slay.fastf ? 1 : 0;
   ra.qsearch = nullptr;
   ra.qprune = nullptr;
   return ra;

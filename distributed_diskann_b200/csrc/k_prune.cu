@@ -59,12 +59,13 @@ __global__ void __launch_bounds__(512) k_prune(IndexView ix, RoundArgs ra, Prune
     // the visited list, sorted by (dist, id) like the reference's
     const uint32_t* vis = ra.vis_all + b * 2ull * vcap;
     uint32_t m = min(ra.stat_vis[b], vcap);
+    const uint32_t off = ra.vis_sorted_tail ? vcap - m : 0u;
     for (uint32_t j = lane; j < m; j += 32) {
-      Pm.cid[j] = vis[j];
-      Pm.ckey[j] = __uint_as_float(vis[vcap + j]);
+      Pm.cid[j] = vis[off + j];
+      Pm.ckey[j] = __uint_as_float(vis[vcap + off + j]);
     }
     __syncwarp();
-    warp_sort_pairs(Pm.cid, Pm.ckey, m);
+    if (!ra.vis_sorted_tail) warp_sort_pairs(Pm.cid, Pm.ckey, m);
     // robustPrune adds p's current out-list (round-start snapshot)
     const uint32_t* prow = ix.graph + (uint64_t)p * ix.Rp;
     for (uint32_t b0 = 0; b0 < ix.Rp; b0 += 32) {

@@ -71,6 +71,8 @@ struct RoundArgs {
   uint32_t* stat_vis;    // B visited-list lengths (k_search writes, k_prune reads)
   uint32_t* stat_cmps;   // B (may be null)
   uint32_t* vis_all;     // per batch point: vcap visited ids, then vcap distances
+  int vis_sorted_tail;   // 1: each list is already in (dist, id) order at the end of its
+                         // slice (the fast search's layout); 0: visit order from the start
   // device work queues (zeroed before the round): with a queue the launch is
   // persistent and each warp takes its next batch point from the counter;
   // null = static grid-stride assignment

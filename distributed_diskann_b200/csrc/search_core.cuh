@@ -200,6 +200,10 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
   uint32_t fr_n = 1;
   uint32_t scan0 = 0;      // lower bound of the first unvisited frontier position
   uint32_t vis_n = 0;      // visited list length
+  // Fast form: the visited list is built sorted, from the end of its slice
+  // down (see the eviction step), so it leaves the search in the reference's
+  // (dist, id) order with no sort: [vtop, vcap) holds it.
+  uint32_t vtop = P.vcap;
   uint32_t ev_n = 0;       // evicted list length (query mode)
   uint32_t cmps = 1;       // dist to the start point
   uint64_t num_visited = 0;
@@ -249,7 +253,7 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
     __syncwarp();
     if (lane == 0) {
       S.fr_id[cur_pos] = cur | DD_VBIT;
-      if (P.keep_visited) {
+      if (P.keep_visited && !FASTF) {
         if (vis_n < P.vcap) {
           S.vis_id[vis_n] = cur;
           S.vis_d[vis_n] = cur_d;
@@ -258,7 +262,7 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
         }
       }
     }
-    if (P.keep_visited && vis_n < P.vcap) vis_n++;
+    if (P.keep_visited && (FASTF || vis_n < P.vcap)) vis_n++;
     num_visited++;
     // the next unvisited entry after cur: visited next unless a new candidate beats it
     int nxt_pos = -1;
@@ -542,6 +546,40 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
         S.fr_d[c_pos[t]] = c_ds[t];
       }
     }
+    if (FASTF && P.keep_visited) {
+      // Visited entries pushed off the end of a full frontier never come back
+      // in a build search (they fail the cutoff from now on), and every entry
+      // pushed off later is smaller in (dist, id) than every one pushed off
+      // before (the frontier's last entry only improves, and candidates must
+      // beat it).  So each block, in frontier order, goes just below the
+      // blocks already written; the final frontier's visited entries go below
+      // them at the end.
+      uint32_t emask[FPL];
+      uint32_t etot = 0;
+#pragma unroll
+      for (int t = 0; t < FPL; t++) {
+        const bool ev = (my_pos[t] != DD_NONE) && (my_pos[t] >= new_n) && (my_id[t] & DD_VBIT);
+        emask[t] = __ballot_sync(FULL, ev);
+        etot += __popc(emask[t]);
+      }
+      if (etot > vtop) {
+        if (lane == 0) dd_set_error(P.err, DD_EVIS_CAP);
+        vtop = 0;
+      } else if (etot) {
+        const uint32_t base = vtop - etot;
+        uint32_t acc = 0;
+#pragma unroll
+        for (int t = 0; t < FPL; t++) {
+          if ((emask[t] >> lane) & 1u) {
+            const uint32_t pos = base + acc + __popc(emask[t] & lanemask_lt());
+            S.vis_id[pos] = my_id[t] & ~DD_VBIT;
+            S.vis_d[pos] = my_d[t];
+          }
+          acc += __popc(emask[t]);
+        }
+        vtop = base;
+      }
+    }
     if (P.query_mode) {
       // visited entries pushed off the end are remembered (in frontier order)
 #pragma unroll
@@ -597,9 +635,37 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
       __syncwarp();
     }
   }
+  if (FASTF && P.keep_visited) {
+    // the final frontier's visited entries, in order, below the evicted blocks
+    uint32_t nflag = 0;
+    for (uint32_t base = 0; base < fr_n; base += 32) {
+      const uint32_t i = base + lane;
+      nflag += __popc(__ballot_sync(FULL, i < fr_n && (S.fr_id[i] & DD_VBIT)));
+    }
+    if (nflag > vtop) {
+      if (lane == 0) dd_set_error(P.err, DD_EVIS_CAP);
+      vtop = 0;
+    } else {
+      uint32_t pos0 = vtop - nflag;
+      for (uint32_t base = 0; base < fr_n; base += 32) {
+        const uint32_t i = base + lane;
+        const bool f = i < fr_n && (S.fr_id[i] & DD_VBIT);
+        const uint32_t fb = __ballot_sync(FULL, f);
+        if (f) {
+          const uint32_t pos = pos0 + __popc(fb & lanemask_lt());
+          S.vis_id[pos] = S.fr_id[i] & ~DD_VBIT;
+          S.vis_d[pos] = S.fr_d[i];
+        }
+        pos0 += __popc(fb);
+      }
+      vtop -= nflag;
+    }
+    __syncwarp();
+  }
   SearchOut o;
   o.fr_n = fr_n;
-  o.vis_n = P.keep_visited ? vis_n : (uint32_t)num_visited;
+  // fast form: the recorded list [vtop, vcap), whose length is the visit count
+  o.vis_n = !P.keep_visited ? (uint32_t)num_visited : (FASTF ? P.vcap - vtop : vis_n);
   o.cmps = cmps;
   return o;
 }
