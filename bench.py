@@ -61,6 +61,10 @@ def parse():
                     help="queries of the reference's timed query sweep")
     ap.add_argument("--plain-steps", type=int, default=3,
                     help="timed builds of the plain exact form (capped by --steps)")
+    ap.add_argument("--nvtx-build", action="store_true",
+                    help="profiling run: calibrate the fast form's shapes on a 100k-point index "
+                         "of the workload, then one instrumented fast build of --n points inside "
+                         "the NVTX range 'target' (for ncu --nvtx-include target/); prints stats")
     ap.add_argument("--sharded", action="store_true",
                     help="with N ranks: one build spread over the N GPUs (the reference's "
                          "distributed build; NCCL all-gathers), instead of N independent builds")
@@ -289,6 +293,35 @@ def run_sharded(args, rank, world, local_rank):
     gi.close()
 
 
+# ---------------------------------------------------------------------- profiling run
+def run_nvtx_build(args):
+    """Calibrates the autotuner on a 100k-point index of the same shape (its
+    shapes are cached per shape, not per n), then runs one fast build with
+    statistics inside the NVTX range 'target': the build's k_search launch of
+    round r is then the r-th k_search launch of that range."""
+    import torch
+
+    from distributed_diskann_b200 import datasets as D
+    from distributed_diskann_b200.index import GpuIndex
+
+    w = D.WORKLOADS[args.workload]
+    b0, _ = D.make_workload(w, n=min(100_000, w.n), nq=1)
+    g0 = GpuIndex(b0.dtype, w.metric, b0.shape[0], w.d, w.R)
+    g0.upload_points(b0)
+    g0.build(w.L, w.alpha, mode="fast")
+    g0.close()
+    n = args.n or w.n
+    base, _ = D.make_workload(w, n=n, nq=1)
+    gi = GpuIndex(base.dtype, w.metric, n, w.d, w.R)
+    gi.upload_points(base)
+    torch.cuda.nvtx.range_push("target")
+    st = gi.build(w.L, w.alpha, mode="fast", collect_stats=True)
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    print(json.dumps({"nvtx_build": st, "n": n, "workload": w.name}), flush=True)
+    gi.close()
+
+
 # ---------------------------------------------------------------------- our arm
 def main():
     args = parse()
@@ -297,6 +330,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.nvtx_build:
+        run_nvtx_build(args)
         return
 
     import torch
