@@ -86,10 +86,8 @@ __device__ void reverse_one(const IndexView& ix, const RoundArgs& ra, const Reve
   __syncwarp();
   const uint32_t m = s + deg;
   warp_std_sort(Pm, m);
-  // plain form: the candidate rows were just read for their distances to t,
-  // so no prefetch; the fast form took the sources' distances from their
-  // prunes, so their rows are not in cache: the next chunk is loaded early
-  warp_greedy_select_fast<DT, MT, TC, TC>(ix.points, ix.stride, ix.d, t, Pm, m, ra.alpha, ix.R, row,
+  // the candidate rows were just read for their distances to t: no prefetch
+  warp_greedy_select_fast<DT, MT, false, TC>(ix.points, ix.stride, ix.d, t, Pm, m, ra.alpha, ix.R, row,
                                          ix.Rp, Pm.sel);
   if (lane == 0) {
     atomicAdd(&rs.counters[2], 1u);
