@@ -377,160 +377,244 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
       continue;
     }
 
-    // ---- rank candidates by (dist, id).  The same id can be kept twice in one
-    // step (a row holding it twice, with a colliding id between the copies,
-    // defeats the lossy filter); identical copies keep their index order.
-    for (uint32_t i = lane; i < nc; i += 32) {
-      float di = S.c_d[i];
-      uint32_t ii = S.c_id[i];
-      uint32_t r = 0;
-      for (uint32_t j = 0; j < nc; j++) {
-        float dj = S.c_d[j];
-        uint32_t ij = S.c_id[j];
-        // (the fast form's rows hold no repeated id, so no identical copies)
-        r += (pair_less(dj, ij, di, ii) || (!FASTF && dj == di && ij == ii && j < i)) ? 1u : 0u;
-      }
-      S.s_id[r] = ii;
-      S.s_d[r] = di;
-    }
-    __syncwarp();
-    // set_union as multisets: with m frontier copies of a value and n candidate
-    // copies, the candidate copies k >= m are added, after the frontier's copies.
-    // A re-entering copy counts as visited while k < (visits of the value):
-    // set_difference(frontier, visited) is a multiset difference too.
-    bool a_ok[CPL];
-    uint32_t a_id[CPL], a_ub[CPL];
-    float a_d[CPL];
-#pragma unroll
-    for (int t = 0; t < CPL; t++) {
-      uint32_t i = lane + 32 * t;
-      a_ok[t] = false;
-      a_id[t] = 0;
-      a_ub[t] = 0;
-      a_d[t] = 0.f;
-      if (i < nc) {
-        uint32_t ci = S.s_id[i];
-        float cd = S.s_d[i];
-        uint32_t k = 0;  // index of this copy among identical candidates
-        for (uint32_t u = i; u > 0 && S.s_id[u - 1] == ci && S.s_d[u - 1] == cd; u--) k++;
-        uint32_t lo = 0, hi = fr_n;
+    // Every step ends with the same scatter: frontier entry t of this lane
+    // moves to my_pos[t] (DD_NONE: no entry), candidate slot t to c_pos[t].
+    uint32_t nkeep = 0, ub0 = 0;
+    uint32_t my_id[FPL], my_pos[FPL];
+    float my_d[FPL];
+    uint32_t c_ids[CPL], c_pos[CPL];
+    float c_ds[CPL];
+    if (FASTF && nc <= 32) {
+      // ---- Fast form with at most 32 candidates (nearly every step): one
+      // candidate per lane, ordered with shuffles, no shared-memory round
+      // trips.  Its rows hold no repeated id and it only runs build searches
+      // (no evicted list, no k-cut), so the candidates are distinct, the
+      // frontier holds each id at most once, and a candidate is added unless
+      // the frontier already holds it.
+      const bool cv = lane < nc;
+      const float cd = cv ? S.c_d[lane] : 0.f;
+      const uint32_t ci = cv ? S.c_id[lane] : 0u;
+      uint32_t lo = 0;  // frontier entries below this candidate
+      bool keep = false;
+      if (cv) {
+        uint32_t hi = fr_n;
         while (lo < hi) {
-          uint32_t mid = (lo + hi) >> 1;
+          const uint32_t mid = (lo + hi) >> 1;
           if (pair_less(S.fr_d[mid], S.fr_id[mid] & ~DD_VBIT, cd, ci)) lo = mid + 1;
           else hi = mid;
         }
-        uint32_t ub = lo, mf = 0;
-        while (ub < fr_n && S.fr_d[ub] == cd && (S.fr_id[ub] & ~DD_VBIT) == ci) {
-          mf += (S.fr_id[ub] & DD_VBIT) ? 1u : 0u;
-          ub++;
-        }
-        const uint32_t m = ub - lo;
-        if (k >= m) {
-          a_ok[t] = true;
-          if (P.query_mode) {
-            uint32_t ev = 0;
-            if (ev_bloom_maybe(S.ev_bloom, ci))
-              for (uint32_t e = 0; e < ev_n; e++) ev += (S.ev_id[e] == ci) ? 1u : 0u;
-            if (k < mf + ev) ci |= DD_VBIT;
-          }
-          a_id[t] = ci;
-          a_d[t] = cd;
-          a_ub[t] = ub;
-        }
+        keep = !(lo < fr_n && S.fr_d[lo] == cd && (S.fr_id[lo] & ~DD_VBIT) == ci);
       }
-    }
-    __syncwarp();
-    uint32_t nkeep = 0;
+      const uint32_t K = __ballot_sync(FULL, keep);
+      nkeep = __popc(K);
+      // one pass over the kept candidates gives this candidate's rank among
+      // them and each frontier entry's shift (#kept candidates placed before it)
+      uint32_t krank = 0;
+      uint32_t shift[FPL];
 #pragma unroll
-    for (int t = 0; t < CPL; t++) {
-      uint32_t ob = __ballot_sync(FULL, a_ok[t]);
-      if (a_ok[t]) {
-        uint32_t pos = nkeep + __popc(ob & lanemask_lt());
-        // c_* become the kept candidates in sorted order; s_id their frontier upper bound
-        S.c_id[pos] = a_id[t];
-        S.c_d[pos] = a_d[t];
-        S.s_id[pos] = a_ub[t];
+      for (int t = 0; t < FPL; t++) shift[t] = 0;
+      for (uint32_t km = K; km; km &= km - 1) {
+        const uint32_t k = __ffs(km) - 1;
+        const float dk = __shfl_sync(FULL, cd, k);
+        const uint32_t ik = __shfl_sync(FULL, ci, k);
+        const uint32_t lk = __shfl_sync(FULL, lo, k);
+        krank += pair_less(dk, ik, cd, ci) ? 1u : 0u;
+#pragma unroll
+        for (int t = 0; t < FPL; t++) shift[t] += (lk <= lane + 32u * t) ? 1u : 0u;
       }
-      nkeep += __popc(ob);
-    }
-    __syncwarp();
-    {
-      // expected next node: the better of the best new candidate and nxt_pos
-      uint32_t nid = DD_NONE;
-      if (nkeep > 0 && !(S.c_id[0] & DD_VBIT)) nid = S.c_id[0];
-      if (nxt_pos >= 0 &&
-          (nid == DD_NONE || !pair_less(S.c_d[0], nid, S.fr_d[nxt_pos], S.fr_id[nxt_pos])))
-        nid = S.fr_id[nxt_pos];
-      if (nid != DD_NONE) prefetch_row(nid);
-    }
-    if (nkeep == 0) {
-      scan0 = nxt_pos >= 0 ? (uint32_t)nxt_pos : fr_n;
-      continue;
-    }
+      {
+        // expected next node: the better of the best new candidate and nxt_pos
+        uint32_t nid = DD_NONE;
+        float nd = 0.f;
+        if (K) {
+          const uint32_t src = __ffs(__ballot_sync(FULL, keep && krank == 0)) - 1;
+          nid = __shfl_sync(FULL, ci, src);
+          nd = __shfl_sync(FULL, cd, src);
+        }
+        if (nxt_pos >= 0 &&
+            (nid == DD_NONE || !pair_less(nd, nid, S.fr_d[nxt_pos], S.fr_id[nxt_pos])))
+          nid = S.fr_id[nxt_pos];
+        if (nid != DD_NONE) prefetch_row(nid);
+      }
+      if (nkeep == 0) {
+        scan0 = nxt_pos >= 0 ? (uint32_t)nxt_pos : fr_n;
+        continue;
+      }
+      ub0 = __reduce_min_sync(FULL, keep ? lo : 0xFFFFFFFFu);
+#pragma unroll
+      for (int t = 0; t < FPL; t++) {
+        const uint32_t i = lane + 32 * t;
+        my_pos[t] = DD_NONE;
+        my_id[t] = 0;
+        my_d[t] = 0.f;
+        if (i < fr_n) {
+          my_pos[t] = i + shift[t];  // entries before ub0 have no shift: not rewritten
+          if (i >= ub0) {
+            my_id[t] = S.fr_id[i];
+            my_d[t] = S.fr_d[i];
+          }
+        }
+      }
+      c_ids[0] = ci;
+      c_ds[0] = cd;
+      c_pos[0] = keep ? lo + krank : DD_NONE;
+#pragma unroll
+      for (int t = 1; t < CPL; t++) {
+        c_ids[t] = 0;
+        c_ds[t] = 0.f;
+        c_pos[t] = DD_NONE;
+      }
+    } else {
+      // ---- rank candidates by (dist, id).  The same id can be kept twice in one
+      // step (a row holding it twice, with a colliding id between the copies,
+      // defeats the lossy filter); identical copies keep their index order.
+      for (uint32_t i = lane; i < nc; i += 32) {
+        float di = S.c_d[i];
+        uint32_t ii = S.c_id[i];
+        uint32_t r = 0;
+        for (uint32_t j = 0; j < nc; j++) {
+          float dj = S.c_d[j];
+          uint32_t ij = S.c_id[j];
+          // (the fast form's rows hold no repeated id, so no identical copies)
+          r += (pair_less(dj, ij, di, ii) || (!FASTF && dj == di && ij == ii && j < i)) ? 1u : 0u;
+        }
+        S.s_id[r] = ii;
+        S.s_d[r] = di;
+      }
+      __syncwarp();
+      // set_union as multisets: with m frontier copies of a value and n candidate
+      // copies, the candidate copies k >= m are added, after the frontier's copies.
+      // A re-entering copy counts as visited while k < (visits of the value):
+      // set_difference(frontier, visited) is a multiset difference too.
+      bool a_ok[CPL];
+      uint32_t a_id[CPL], a_ub[CPL];
+      float a_d[CPL];
+#pragma unroll
+      for (int t = 0; t < CPL; t++) {
+        uint32_t i = lane + 32 * t;
+        a_ok[t] = false;
+        a_id[t] = 0;
+        a_ub[t] = 0;
+        a_d[t] = 0.f;
+        if (i < nc) {
+          uint32_t ci = S.s_id[i];
+          float cd = S.s_d[i];
+          uint32_t k = 0;  // index of this copy among identical candidates
+          for (uint32_t u = i; u > 0 && S.s_id[u - 1] == ci && S.s_d[u - 1] == cd; u--) k++;
+          uint32_t lo = 0, hi = fr_n;
+          while (lo < hi) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (pair_less(S.fr_d[mid], S.fr_id[mid] & ~DD_VBIT, cd, ci)) lo = mid + 1;
+            else hi = mid;
+          }
+          uint32_t ub = lo, mf = 0;
+          while (ub < fr_n && S.fr_d[ub] == cd && (S.fr_id[ub] & ~DD_VBIT) == ci) {
+            mf += (S.fr_id[ub] & DD_VBIT) ? 1u : 0u;
+            ub++;
+          }
+          const uint32_t m = ub - lo;
+          if (k >= m) {
+            a_ok[t] = true;
+            if (P.query_mode) {
+              uint32_t ev = 0;
+              if (ev_bloom_maybe(S.ev_bloom, ci))
+                for (uint32_t e = 0; e < ev_n; e++) ev += (S.ev_id[e] == ci) ? 1u : 0u;
+              if (k < mf + ev) ci |= DD_VBIT;
+            }
+            a_id[t] = ci;
+            a_d[t] = cd;
+            a_ub[t] = ub;
+          }
+        }
+      }
+      __syncwarp();
+#pragma unroll
+      for (int t = 0; t < CPL; t++) {
+        uint32_t ob = __ballot_sync(FULL, a_ok[t]);
+        if (a_ok[t]) {
+          uint32_t pos = nkeep + __popc(ob & lanemask_lt());
+          // c_* become the kept candidates in sorted order; s_id their frontier upper bound
+          S.c_id[pos] = a_id[t];
+          S.c_d[pos] = a_d[t];
+          S.s_id[pos] = a_ub[t];
+        }
+        nkeep += __popc(ob);
+      }
+      __syncwarp();
+      {
+        // expected next node: the better of the best new candidate and nxt_pos
+        uint32_t nid = DD_NONE;
+        if (nkeep > 0 && !(S.c_id[0] & DD_VBIT)) nid = S.c_id[0];
+        if (nxt_pos >= 0 &&
+            (nid == DD_NONE || !pair_less(S.c_d[0], nid, S.fr_d[nxt_pos], S.fr_id[nxt_pos])))
+          nid = S.fr_id[nxt_pos];
+        if (nid != DD_NONE) prefetch_row(nid);
+      }
+      if (nkeep == 0) {
+        scan0 = nxt_pos >= 0 ? (uint32_t)nxt_pos : fr_n;
+        continue;
+      }
 
-    // ---- merge: frontier entry i moves to i + #(kept candidates placed before
-    // it) = i + #{j : ub_j <= i}; candidate j moves to j + ub_j.  Entries
-    // before the first insertion point ub_0 stay where they are.
+      // ---- merge: frontier entry i moves to i + #(kept candidates placed before
+      // it) = i + #{j : ub_j <= i}; candidate j moves to j + ub_j.  Entries
+      // before the first insertion point ub_0 stay where they are.
+      ub0 = S.s_id[0];
+      // Fast form with few kept candidates (the common case once the frontier
+      // is full): every entry's shift is counted from the broadcast ub_j, with
+      // no per-entry binary search.
+      const bool count_shift = FASTF && nkeep <= 8;
+      uint32_t shift[FPL];
+#pragma unroll
+      for (int t = 0; t < FPL; t++) shift[t] = 0;
+      if (count_shift) {
+        for (uint32_t j = 0; j < nkeep; j++) {
+          const uint32_t ubj = S.s_id[j];
+#pragma unroll
+          for (int t = 0; t < FPL; t++) shift[t] += (ubj <= lane + 32u * t) ? 1u : 0u;
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < FPL; t++) {
+        uint32_t i = lane + 32 * t;
+        my_pos[t] = DD_NONE;
+        my_id[t] = 0;
+        my_d[t] = 0.f;
+        if (i < fr_n) {
+          if (i < ub0) {
+            my_pos[t] = i;  // unmoved: not rewritten
+          } else {
+            uint32_t lo = shift[t];
+            if (!count_shift) {
+              uint32_t hi = nkeep;
+              lo = 1;
+              while (lo < hi) {
+                uint32_t mid = (lo + hi) >> 1;
+                if (S.s_id[mid] <= i) lo = mid + 1;
+                else hi = mid;
+              }
+            }
+            my_id[t] = S.fr_id[i];
+            my_d[t] = S.fr_d[i];
+            my_pos[t] = i + lo;
+          }
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < CPL; t++) {
+        uint32_t j = lane + 32 * t;
+        c_pos[t] = DD_NONE;
+        c_ids[t] = 0;
+        c_ds[t] = 0.f;
+        if (j < nkeep) {
+          c_ids[t] = S.c_id[j];
+          c_ds[t] = S.c_d[j];
+          c_pos[t] = j + S.s_id[j];
+        }
+      }
+    }
     const uint32_t new_n = min(P.L, fr_n + nkeep);
-    const uint32_t ub0 = S.s_id[0];
     // unvisited entries now sit at or after min(ub_0, old nxt_pos)
     scan0 = min(ub0, nxt_pos >= 0 ? (uint32_t)nxt_pos : new_n);
-    uint32_t my_id[FPL], my_pos[FPL];
-    float my_d[FPL];
-    // Fast form with few kept candidates (the common case once the frontier
-    // is full): every entry's shift is counted from the broadcast ub_j, with
-    // no per-entry binary search.
-    const bool count_shift = FASTF && nkeep <= 8;
-    uint32_t shift[FPL];
-#pragma unroll
-    for (int t = 0; t < FPL; t++) shift[t] = 0;
-    if (count_shift) {
-      for (uint32_t j = 0; j < nkeep; j++) {
-        const uint32_t ubj = S.s_id[j];
-#pragma unroll
-        for (int t = 0; t < FPL; t++) shift[t] += (ubj <= lane + 32u * t) ? 1u : 0u;
-      }
-    }
-#pragma unroll
-    for (int t = 0; t < FPL; t++) {
-      uint32_t i = lane + 32 * t;
-      my_pos[t] = DD_NONE;
-      my_id[t] = 0;
-      my_d[t] = 0.f;
-      if (i < fr_n) {
-        if (i < ub0) {
-          my_pos[t] = i;  // unmoved: not rewritten
-        } else {
-          uint32_t lo = shift[t];
-          if (!count_shift) {
-            uint32_t hi = nkeep;
-            lo = 1;
-            while (lo < hi) {
-              uint32_t mid = (lo + hi) >> 1;
-              if (S.s_id[mid] <= i) lo = mid + 1;
-              else hi = mid;
-            }
-          }
-          my_id[t] = S.fr_id[i];
-          my_d[t] = S.fr_d[i];
-          my_pos[t] = i + lo;
-        }
-      }
-    }
-    uint32_t c_ids[CPL], c_pos[CPL];
-    float c_ds[CPL];
-#pragma unroll
-    for (int t = 0; t < CPL; t++) {
-      uint32_t j = lane + 32 * t;
-      c_pos[t] = DD_NONE;
-      c_ids[t] = 0;
-      c_ds[t] = 0.f;
-      if (j < nkeep) {
-        c_ids[t] = S.c_id[j];
-        c_ds[t] = S.c_d[j];
-        c_pos[t] = j + S.s_id[j];
-      }
-    }
     __syncwarp();
 #pragma unroll
     for (int t = 0; t < FPL; t++) {
