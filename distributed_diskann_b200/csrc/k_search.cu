@@ -37,9 +37,9 @@ WarpLayout make_search_layout(uint32_t d, int dtype, uint32_t L, uint32_t Rp, ui
   w.s_d = off; off += r16(4ull * Rp);
   w.vcap = vcap;
   w.ccap = vcap + Rp;
-  w.hbits = hash_bits_for(L);
-  w.h24 = h24 ? 1u : 0u;
   w.fastf = (build && fastf) ? 1u : 0u;
+  w.hbits = w.fastf ? fast_hash_bits(L) : hash_bits_for(L);
+  w.h24 = h24 ? 1u : 0u;
   const uint32_t hash_bytes =
       r16(w.fastf ? fast_table_bytes(w.hbits) : hash_table_bytes(w.hbits, h24));
   if (build) {

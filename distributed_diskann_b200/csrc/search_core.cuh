@@ -63,14 +63,17 @@ __host__ __device__ inline uint32_t hash_table_bytes(uint32_t hbits, bool h24) {
 // rows_without_repeats).  In a build search (k = 0, no k-cut) the filter
 // only decides which neighbours get their distance computed: an id it lets
 // through twice is re-evaluated, fails the cutoff or is already in the
-// frontier, and set_union drops the copy.  So any filter without false positives gives the
-// reference's frontier, visited list and graph; only the dist_cmps count
-// moves.  This one keeps 2^hbits slots like the reference's, but hashes ids
-// with a bijection of [0, 2^24) and stores the 24 - hbits quotient bits in a
-// 16-bit tag: 2 bytes a slot instead of 3, and a lookup + insert with no
-// same-slot grouping (all lanes read their slots, then the lanes that
-// missed write: a lane that loses a write race only causes a later
-// re-evaluation).
+// frontier, and set_union drops the copy.  So any filter without false
+// positives gives the reference's frontier, visited list and graph; only the
+// dist_cmps count moves.  This one holds 2^hbits 16-bit tags (2 bytes a slot
+// where the reference's table takes 3), set associative: ids are hashed with
+// a bijection of [0, 2^24); the low hbits - 2 bits pick a bucket of four tags
+// (one 8-byte word) and the remaining 26 - hbits bits are the tag, so a tag
+// names exactly one id.  A lookup is one read per lane; a lane that missed
+// pushes its tag into the front of the bucket and the oldest tag falls out.
+// Lanes that write the same bucket in one step race, and the loser's tag is
+// lost: the table only ever holds ids that were evaluated, so a lost tag
+// costs a later re-evaluation, never a wrong answer.
 // ---------------------------------------------------------------------------
 __host__ __device__ inline uint32_t fast_table_bytes(uint32_t hbits) { return 2u << hbits; }
 
@@ -166,6 +169,13 @@ __host__ __device__ inline uint32_t hash_bits_for(uint32_t L) {
   return (uint32_t)(b < 10 ? 10 : b);
 }
 
+// slots of the fast filter: the reference's count, at least 2^11 so that a
+// tag (26 - hbits bits) stays below the empty marker 0xFFFF
+__host__ __device__ inline uint32_t fast_hash_bits(uint32_t L) {
+  const uint32_t b = hash_bits_for(L);
+  return b < 11 ? 11u : b;
+}
+
 template <int DT, int MT>
 __device__ __forceinline__ float point_dist(const SearchParams& P, const uint8_t* qv, uint32_t id) {
   return Dist<DT, MT>::eval(qv, P.points + (uint64_t)id * P.stride, P.d);
@@ -184,7 +194,7 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
   const uint32_t hmask = nslots - 1;
   {
     // all-ones bytes are the empty marker of every layout (a 16-bit tag of
-    // the fast filter is below 2^14)
+    // the fast filter is below 2^15)
     uint4* h4 = (uint4*)S.hash;
     const uint4 none = make_uint4(DD_NONE, DD_NONE, DD_NONE, DD_NONE);
     const uint32_t n16 =
@@ -285,9 +295,10 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
     // written chunk after chunk.
     bool keep[CPL];
     if (FASTF) {
-      uint16_t* tab = (uint16_t*)S.hash;
+      uint2* tab = (uint2*)S.hash;
+      const uint32_t bbits = P.hbits - 2;
       uint32_t slot[CPL];
-      uint16_t tag[CPL];
+      uint2 nw[CPL];
 #pragma unroll
       for (int t = 0; t < CPL; t++) {
         uint32_t at = a[t];
@@ -297,14 +308,18 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
           a[t] = DD_NONE;
         }
         const uint32_t f = mix24(at);
-        slot[t] = f & hmask;
-        tag[t] = (uint16_t)(f >> P.hbits);
-        keep[t] = (at != DD_NONE) && ((uint64_t)at != self_id) && tab[slot[t]] != tag[t];
+        slot[t] = f & ((1u << bbits) - 1u);
+        const uint32_t tag = f >> bbits;
+        const uint32_t tt = tag | (tag << 16);
+        const uint2 w = tab[slot[t]];
+        const bool hit = (__vcmpeq2(w.x, tt) | __vcmpeq2(w.y, tt)) != 0u;
+        keep[t] = (at != DD_NONE) && ((uint64_t)at != self_id) && !hit;
+        nw[t] = make_uint2((w.x << 16) | tag, (w.y << 16) | (w.x >> 16));
       }
       __syncwarp();
 #pragma unroll
       for (int t = 0; t < CPL; t++)
-        if (keep[t]) tab[slot[t]] = tag[t];
+        if (keep[t]) tab[slot[t]] = nw[t];
       __syncwarp();
     } else {
       bool part[CPL];
