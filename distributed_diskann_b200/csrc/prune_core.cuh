@@ -148,6 +148,89 @@ __device__ __forceinline__ void warp_partition_loop(const ddsort::Arr<uint32_t>&
 // otherwise each element's rank (count of smaller keys) is its position, and
 // the list is rewritten through the rank-pairing scratch (2 * cap ints).
 constexpr uint32_t kRankSortMax = 256;
+
+// The rank sort of a list made of one long strictly ascending run and at most
+// 32 other elements: a reverse prune's list, where the target's row is the
+// selection of its last prune (ascending) followed by the few sources
+// appended since, and the new sources come in batch order.  A run element's
+// rank is its place in the run plus the other elements below it; another
+// element's rank is its lower bound in the run (binary search) plus the other
+// elements below it.  Returns 1 when sorted, 0 when two keys are equal (list
+// untouched), -1 when the list does not have that shape (list untouched).
+__device__ __forceinline__ int warp_sort_run_plus_few(const PruneSmem& S, uint32_t m) {
+  const uint32_t FULL = 0xffffffffu;
+  const uint32_t lane = lane_id();
+  constexpr uint32_t kMaxRuns = 48;
+  // the longest run [rs, rs + rl): runs start at 0 and where a key is not
+  // above its predecessor
+  uint32_t nruns = 0, prev = 0, rs = 0, rl = 0;
+  for (uint32_t b = 0; b < m && nruns <= kMaxRuns; b += 32) {
+    const uint32_t i = b + lane;
+    const bool st = i < m && i > 0 && !(S.ckey[i - 1] < S.ckey[i]);
+    for (uint32_t bits = __ballot_sync(FULL, st); bits; bits &= bits - 1) {
+      const uint32_t s0 = b + __ffs(bits) - 1;
+      if (s0 - prev > rl) {
+        rl = s0 - prev;
+        rs = prev;
+      }
+      prev = s0;
+      nruns++;
+    }
+  }
+  if (m - prev > rl) {
+    rl = m - prev;
+    rs = prev;
+  }
+  const uint32_t u = m - rl;
+  if (nruns > kMaxRuns || u > 32) return -1;
+  // lane q < u holds the q-th element outside the run
+  const bool qv = lane < u;
+  const uint32_t qi = lane < rs ? lane : lane + rl;
+  const float kq = qv ? S.ckey[qi] : 0.f;
+  const uint32_t re = rs + rl;
+  uint32_t rq = rs;
+  bool tie = false;
+  if (qv) {
+    uint32_t hi = re;
+    while (rq < hi) {
+      const uint32_t mid = (rq + hi) >> 1;
+      if (S.ckey[mid] < kq) rq = mid + 1;
+      else hi = mid;
+    }
+    tie = rq < re && S.ckey[rq] == kq;
+  }
+  rq -= rs;
+  for (uint32_t j = 0; j < u; j++) {
+    const float kj = __shfl_sync(FULL, kq, j);
+    rq += kj < kq ? 1u : 0u;
+    tie |= qv && j != lane && kj == kq;
+  }
+  if (__any_sync(FULL, tie)) return 0;
+  int* tid = S.posL;
+  float* tkey = (float*)S.posR;
+  if (qv) {
+    tid[rq] = (int)S.cid[qi];
+    tkey[rq] = kq;
+  }
+  for (uint32_t b = 0; b < rl; b += 32) {
+    const uint32_t i = b + lane;
+    const float ki = i < rl ? S.ckey[rs + i] : 0.f;
+    uint32_t r = i;
+    for (uint32_t j = 0; j < u; j++) r += __shfl_sync(FULL, kq, j) < ki ? 1u : 0u;
+    if (i < rl) {
+      tid[r] = (int)S.cid[rs + i];
+      tkey[r] = ki;
+    }
+  }
+  __syncwarp();
+  for (uint32_t i = lane; i < m; i += 32) {
+    S.cid[i] = (uint32_t)tid[i];
+    S.ckey[i] = tkey[i];
+  }
+  __syncwarp();
+  return 1;
+}
+
 __device__ __forceinline__ bool warp_sort_distinct(const PruneSmem& S, uint32_t m) {
   const uint32_t FULL = 0xffffffffu;
   const uint32_t lane = lane_id();
@@ -160,6 +243,8 @@ __device__ __forceinline__ bool warp_sort_distinct(const PruneSmem& S, uint32_t 
   }
   if (strict && nondesc) return true;
   if (nondesc || m > kRankSortMax) return false;
+  const int rp = warp_sort_run_plus_few(S, m);
+  if (rp >= 0) return rp == 1;
   uint32_t rk[kRankSortMax / 32];
   bool tie = false;
 #pragma unroll
