@@ -111,11 +111,12 @@ __device__ __forceinline__ SearchSmem carve_query(uint8_t* base, const WarpLayou
 // k_search: one warp per batch point runs beam_search on the round-start graph
 // and leaves its visited list in the point's global slice
 // (include/index.h:274-278; src/bsp_index.hpp:259-268).
-// FASTF: the fast form's seen filter, with registers capped (L <= 128) so
-// that 22 searches (two 11-warp CTAs) fit an SM, the most its shared memory
-// holds at L = 128 with that filter's 8 KB table.
+// FASTF: the fast form's seen filter, with registers capped at 64 (L <= 128)
+// so that four CTAs of up to 8 warps fit an SM; at L = 128 a search takes
+// 6.2 KB of shared memory with that filter's 4 KB table, and the autotuner
+// settles on four 7-warp CTAs (28 searches per SM).
 template <int DT, int MT, int FPL, int CPL, bool FASTF>
-__global__ void __launch_bounds__((FASTF && FPL == 4) ? 352 : 512, (FASTF && FPL == 4) ? 2 : 1)
+__global__ void __launch_bounds__((FASTF && FPL == 4) ? 256 : 512, (FASTF && FPL == 4) ? 4 : 1)
     k_search(IndexView ix, RoundArgs ra, WarpLayout lay) {
   extern __shared__ uint4 smem_raw[];
   const uint32_t wpc = blockDim.x >> 5;

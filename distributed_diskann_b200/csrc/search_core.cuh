@@ -169,10 +169,12 @@ __host__ __device__ inline uint32_t hash_bits_for(uint32_t L) {
   return (uint32_t)(b < 10 ? 10 : b);
 }
 
-// slots of the fast filter: the reference's count, at least 2^11 so that a
-// tag (26 - hbits bits) stays below the empty marker 0xFFFF
+// slots of the fast filter: half the reference's count (the four-way buckets
+// keep tags longer than its one-id slots, and the smaller table lets more
+// searches share an SM), at least 2^11 so that a tag (26 - hbits bits) stays
+// below the empty marker 0xFFFF
 __host__ __device__ inline uint32_t fast_hash_bits(uint32_t L) {
-  const uint32_t b = hash_bits_for(L);
+  const uint32_t b = hash_bits_for(L) - 1;
   return b < 11 ? 11u : b;
 }
 
