@@ -550,9 +550,10 @@ def main():
             "config": {"workload": f"{w.name}: {n}x{w.d} {w.dtype} {w.metric}, R={w.R}, "
                                    f"L={w.L}, alpha={w.alpha} (full batched build per step)",
                        "n": n, "d": w.d, "R": w.R, "L": w.L, "alpha": w.alpha,
-                       "form": "fast (INT8 tensor-core prune tiles, persistent work-queue "
-                               "kernels, CUDA-graph build replay, autotuned CTA shapes); graph "
-                               "bit-exact vs the reference build",
+                       "form": "fast (INT8 tensor-core prune tiles, set-associative seen "
+                               "filter and register step merges in the build search, "
+                               "persistent work-queue kernels, CUDA-graph build replay, "
+                               "autotuned CTA shapes); graph bit-exact vs the reference build",
                        "l2_flush": "inputs larger than L2 (points + graph > 126 MB)",
                        "parallelism": f"{world} independent partitions" if world > 1 else "1 GPU"},
             "e2e": {"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": h2d,
