@@ -690,14 +690,6 @@ __device__ __forceinline__ uint32_t any_over_rows(uint32_t b) {
 __device__ __forceinline__ uint32_t spread4(uint32_t x) {
   return (x & 1u) | ((x & 2u) << 1) | ((x & 4u) << 2) | ((x & 8u) << 3);
 }
-// bits at positions 0, 4, ..., 28 -> bits 0..7
-__device__ __forceinline__ uint32_t gather_nibble_bits(uint32_t x) {
-  x &= 0x11111111u;
-  x = (x | (x >> 3)) & 0x03030303u;
-  x = (x | (x >> 6)) & 0x000F000Fu;
-  x = (x | (x >> 12)) & 0xFFu;
-  return x;
-}
 
 // PREFETCH: load the next chunk's rows while the current chunk's tiles run
 // (worth it when the rows are not in cache yet).
@@ -803,11 +795,15 @@ __device__ uint32_t warp_greedy_select_mma(const uint8_t* points, uint64_t strid
           const int thr = cthr[col];
           const bool oa = g < col && gram_part<MT>(na, acc[nt][e]) <= thr;
           const bool ob = g + 8 < col && gram_part<MT>(nb, acc[nt][2 + e]) <= thr;
-          const uint32_t bl = __ballot_sync(FULL, oa), bh = __ballot_sync(FULL, ob);
+          // column col's occluder bits (rows g and g + 8), OR-ed over the 8
+          // lanes that hold it (lane = 4 g + t); lane tt then has column
+          // 8 nt + 2 tt + e, which every lane takes
+          uint32_t v = (oa ? 1u << g : 0u) | (ob ? 1u << (g + 8) : 0u);
+          v |= __shfl_xor_sync(FULL, v, 4);
+          v |= __shfl_xor_sync(FULL, v, 8);
+          v |= __shfl_xor_sync(FULL, v, 16);
 #pragma unroll
-          for (int tt = 0; tt < 4; tt++)
-            colmask[8 * nt + 2 * tt + e] =
-                gather_nibble_bits(bl >> tt) | (gather_nibble_bits(bh >> tt) << 8);
+          for (int tt = 0; tt < 4; tt++) colmask[8 * nt + 2 * tt + e] = __shfl_sync(FULL, v, tt);
         }
     }
     uint32_t selm = 0, ns = nsel;
