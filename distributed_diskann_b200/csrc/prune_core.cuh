@@ -630,26 +630,40 @@ __device__ __forceinline__ uint4* mma_row_vec(uint32_t* rw, uint32_t r, uint32_t
   return (uint4*)(rw + r * 32u + ((w ^ (r & 7u)) << 2));
 }
 
+// Four 8 x 16-byte tiles of staged rows into registers (ldmatrix .x4): lane l
+// names row `row` of tile l / 8 at 16-byte word `w`; register j then holds
+// bytes 4 (l % 4) .. 4 (l % 4) + 3 of row l / 4 of tile j, which is the
+// m16n8k32 fragment layout of 8-bit operands.
+__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], uint32_t* rw, uint32_t row, uint32_t w) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(mma_row_vec(rw, row, w));
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(a));
+}
+
 // acc[nt] += rows [ra0, ra0+16) x rows [rb0 + 8 nt, rb0 + 8 nt + 8), nt = 0, 1 (KS k-steps)
 template <int DT>
-__device__ __forceinline__ void mma_tile_16x16(const uint32_t* rw, uint32_t ra0, uint32_t rb0,
+__device__ __forceinline__ void mma_tile_16x16(uint32_t* rw, uint32_t ra0, uint32_t rb0,
                                                uint32_t KS, int (&acc)[2][4]) {
-  const uint32_t lane = lane_id(), g = lane >> 2, t = lane & 3;
+  const uint32_t lane = lane_id(), mi = lane >> 3, ri = lane & 7;
 #pragma unroll
   for (int nt = 0; nt < 2; nt++)
 #pragma unroll
     for (int i = 0; i < 4; i++) acc[nt][i] = 0;
   for (uint32_t ks = 0; ks < KS; ks++) {
-    const uint32_t q = 8 * ks + t;
+    // A: tiles (rows 0-7, k 0-15), (rows 8-15, k 0-15), (rows 0-7, k 16-31), (rows 8-15, k 16-31)
     uint32_t a[4];
-    a[0] = mma_row_word(rw, ra0 + g, q);
-    a[1] = mma_row_word(rw, ra0 + g + 8, q);
-    a[2] = mma_row_word(rw, ra0 + g, q + 4);
-    a[3] = mma_row_word(rw, ra0 + g + 8, q + 4);
-#pragma unroll
-    for (int nt = 0; nt < 2; nt++) {
-      const uint32_t rb = rb0 + 8 * nt + g;
-      mma_k32<DT>(acc[nt], a, mma_row_word(rw, rb, q), mma_row_word(rw, rb, q + 4));
+    ldsm_x4(a, rw, ra0 + (mi & 1u) * 8u + ri, 2u * ks + (mi >> 1));
+    if (ra0 == rb0) {
+      // the chunk's own tile: B's n-tiles are A's row halves
+      mma_k32<DT>(acc[0], a, a[0], a[2]);
+      mma_k32<DT>(acc[1], a, a[1], a[3]);
+    } else {
+      // B: tiles (rows 0-7, k 0-15), (rows 0-7, k 16-31), (rows 8-15, k 0-15), (rows 8-15, k 16-31)
+      uint32_t b[4];
+      ldsm_x4(b, rw, rb0 + (mi >> 1) * 8u + ri, 2u * ks + (mi & 1u));
+      mma_k32<DT>(acc[0], a, b[0], b[1]);
+      mma_k32<DT>(acc[1], a, b[2], b[3]);
     }
   }
 }
@@ -678,18 +692,6 @@ __device__ __forceinline__ int gram_part(int na, int dot) {
   return MT == DD_L2 ? na - 2 * dot : -dot;
 }
 
-// OR over the 8 rows of a ballot of fragment elements (lane = 4 g + t):
-// returns 4 bits, bit t set when some lane with that t voted
-__device__ __forceinline__ uint32_t any_over_rows(uint32_t b) {
-  b |= b >> 16;
-  b |= b >> 8;
-  b |= b >> 4;
-  return b & 0xFu;
-}
-// bits 0..3 -> bits 0, 2, 4, 6
-__device__ __forceinline__ uint32_t spread4(uint32_t x) {
-  return (x & 1u) | ((x & 2u) << 1) | ((x & 4u) << 2) | ((x & 8u) << 3);
-}
 
 // PREFETCH: load the next chunk's rows while the current chunk's tiles run
 // (worth it when the rows are not in cache yet).
@@ -768,6 +770,8 @@ __device__ uint32_t warp_greedy_select_mma(const uint8_t* points, uint64_t strid
       mma_tile_16x16<DT>(rw, r0, nsel, KS, acc);
       const uint32_t sa = r0 + g, sb = r0 + g + 8;
       const int na = MT == DD_L2 ? norms[sa] : 0, nb = MT == DD_L2 ? norms[sb] : 0;
+      // this lane's four columns (8 nt + 2 t + e) occluded by its rows, OR-ed
+      // over the warp
       uint32_t occ = 0;
 #pragma unroll
       for (int nt = 0; nt < 2; nt++)
@@ -776,9 +780,9 @@ __device__ uint32_t warp_greedy_select_mma(const uint8_t* points, uint64_t strid
           const int thr = cthr[8u * nt + 2u * t + e];
           const bool oa = sa < nsel && gram_part<MT>(na, acc[nt][e]) <= thr;
           const bool ob = sb < nsel && gram_part<MT>(nb, acc[nt][2 + e]) <= thr;
-          occ |= spread4(any_over_rows(__ballot_sync(FULL, oa || ob))) << (8 * nt + e);
+          occ |= (oa || ob) ? 1u << (8u * nt + 2u * t + e) : 0u;
         }
-      amask &= ~occ;
+      amask &= ~__reduce_or_sync(FULL, occ);
     }
     // ---- 3. the chunk's own tile, then in-order selection with bit masks
     uint32_t colmask[kMmaChunk];
