@@ -104,16 +104,21 @@ def test_robust_prune_vs_reference(golden):
     gi.close()
 
 
-@pytest.mark.parametrize("ties", [False, True])
-def test_robust_prune_run_shaped_lists_vs_oracle(oracle_mod, ties):
+@pytest.mark.parametrize("shape", ["runs", "runs_one_tie", "sorted_ties", "dense_ties"])
+def test_robust_prune_run_shaped_lists_vs_oracle(oracle_mod, shape):
     """Candidate lists shaped like a reverse prune's: new sources in batch
     order, then an ascending run (the target's last selection), then a few
     appended sources.  The warp sort ranks these from the run; lists with more
     than 32 elements off the run, or with equal keys, take the other sort
-    paths.  Keys below the points' typical distances leave most candidates
-    unoccluded, so the first R places of the sorted list are all checked.
-    Every result must equal the oracle's robustPrune."""
-    rng = np.random.default_rng(23 if ties else 17)
+    paths.  Lists with equal keys replay the library's introsort, whose order
+    of equal keys the greedy selection depends on; ranges of such a list
+    without tied elements are sorted directly: "sorted_ties" is an insert
+    prune's list (ascending, a few equal neighbours), "dense_ties" has keys
+    from a small range.  Keys below the points' typical distances leave most
+    candidates unoccluded, so the first R places of the sorted list are all
+    checked.  Every result must equal the oracle's robustPrune."""
+    rng = np.random.default_rng({"runs": 17, "runs_one_tie": 23, "sorted_ties": 29,
+                                 "dense_ties": 31}[shape])
     n, d, R = 5000, 64, 64
     base = rng.integers(0, 256, (n, d)).astype(np.uint8)
     gi = GpuIndex(base.dtype, "l2", n, d, R)
@@ -127,9 +132,13 @@ def test_robust_prune_run_shaped_lists_vs_oracle(oracle_mod, ties):
         ids = rng.choice(np.delete(np.arange(n), p), m, replace=False).astype(np.uint32)
         keys = rng.choice(200_000, m, replace=False).astype(np.float32)
         keys[s:s + run] = np.sort(keys[s:s + run])
-        if ties and m > 1 and t % 2 == 0:
+        if shape == "runs_one_tie" and m > 1 and t % 2 == 0:
             a, b = rng.choice(m, 2, replace=False)
             keys[a] = keys[b]
+        elif shape == "sorted_ties":
+            keys = np.sort(rng.integers(0, 4 * m, m)).astype(np.float32)
+        elif shape == "dense_ties":
+            keys = rng.integers(0, max(2, m // 3), m).astype(np.float32) * 50.0
         tasks.append((p, ids, keys))
     outs = gi.robust_prune(tasks, 1.2)
     for t, (p, ids, keys) in enumerate(tasks):
