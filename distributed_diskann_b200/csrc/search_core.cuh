@@ -236,18 +236,34 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
     }
   };
 
+  // Fast form: the register merge knows the next node (the first unvisited
+  // entry of the merged frontier), its position and distance, so the next
+  // step skips the scan.  known_pos: -1 unknown (scan), -2 none left.
+  int known_pos = -1;
+  uint32_t known_id = 0;
+  float known_d = 0.f;
   while (num_visited < P.limit) {
     // ---- closest unvisited frontier entry (every entry before scan0 is visited)
     int cur_pos = -1;
-    for (uint32_t base = scan0 & ~31u; base < fr_n; base += 32) {
-      uint32_t i = base + lane;
-      bool unv = (i < fr_n) && !(S.fr_id[i] & DD_VBIT);
-      uint32_t b = __ballot_sync(FULL, unv);
-      if (b) { cur_pos = (int)(base + __ffs(b) - 1); break; }
+    uint32_t cur;
+    float cur_d;
+    if (FASTF && known_pos != -1) {
+      if (known_pos < 0) break;
+      cur_pos = known_pos;
+      cur = known_id;
+      cur_d = known_d;
+    } else {
+      for (uint32_t base = scan0 & ~31u; base < fr_n; base += 32) {
+        uint32_t i = base + lane;
+        bool unv = (i < fr_n) && !(S.fr_id[i] & DD_VBIT);
+        uint32_t b = __ballot_sync(FULL, unv);
+        if (b) { cur_pos = (int)(base + __ffs(b) - 1); break; }
+      }
+      if (cur_pos < 0) break;
+      cur = S.fr_id[cur_pos];
+      cur_d = S.fr_d[cur_pos];
     }
-    if (cur_pos < 0) break;
-    const uint32_t cur = S.fr_id[cur_pos];
-    const float cur_d = S.fr_d[cur_pos];
+    known_pos = -1;
     const float cutoff = (fr_n < P.L) ? int_max_f : S.fr_d[fr_n - 1];
     // the row of the node being visited: all chunks loaded up front
     uint32_t a[CPL];
@@ -389,7 +405,16 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
     }
     __syncwarp();
     if (nc == 0) {
-      if (nxt_pos >= 0) prefetch_row(S.fr_id[nxt_pos]);
+      if (nxt_pos >= 0) {
+        prefetch_row(S.fr_id[nxt_pos]);
+        if (FASTF) {
+          known_pos = nxt_pos;
+          known_id = S.fr_id[nxt_pos];
+          known_d = S.fr_d[nxt_pos];
+        }
+      } else if (FASTF) {
+        known_pos = -2;
+      }
       scan0 = nxt_pos >= 0 ? (uint32_t)nxt_pos : fr_n;
       continue;
     }
@@ -440,18 +465,40 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
         for (int t = 0; t < FPL; t++) shift[t] += (lk <= lane + 32u * t) ? 1u : 0u;
       }
       {
-        // expected next node: the better of the best new candidate and nxt_pos
-        uint32_t nid = DD_NONE;
+        // the next node: the better of the best new candidate and nxt_pos,
+        // which is the first unvisited entry of the merged frontier; in the
+        // fast form also its merged position (the best candidate lands at its
+        // lower bound, the old entry moves by its shift) unless the trim drops it
+        uint32_t nid = DD_NONE, npos = DD_NONE;
         float nd = 0.f;
         if (K) {
           const uint32_t src = __ffs(__ballot_sync(FULL, keep && krank == 0)) - 1;
           nid = __shfl_sync(FULL, ci, src);
           nd = __shfl_sync(FULL, cd, src);
+          npos = __shfl_sync(FULL, lo, src);
         }
-        if (nxt_pos >= 0 &&
-            (nid == DD_NONE || !pair_less(nd, nid, S.fr_d[nxt_pos], S.fr_id[nxt_pos])))
-          nid = S.fr_id[nxt_pos];
+        if (nxt_pos >= 0) {
+          const uint32_t fid = S.fr_id[nxt_pos];
+          const float fd = S.fr_d[nxt_pos];
+          if (nid == DD_NONE || !pair_less(nd, nid, fd, fid)) {
+            nid = fid;
+            nd = fd;
+            if (FASTF) {
+              const uint32_t tn = (uint32_t)nxt_pos >> 5;
+              uint32_t sh = 0;
+#pragma unroll
+              for (int t = 0; t < FPL; t++)
+                if ((uint32_t)t == tn) sh = shift[t];
+              npos = (uint32_t)nxt_pos + __shfl_sync(FULL, sh, (uint32_t)nxt_pos & 31u);
+            }
+          }
+        }
         if (nid != DD_NONE) prefetch_row(nid);
+        if (FASTF) {
+          known_pos = (nid != DD_NONE && npos < min(P.L, fr_n + nkeep)) ? (int)npos : -2;
+          known_id = nid;
+          known_d = nd;
+        }
       }
       if (nkeep == 0) {
         scan0 = nxt_pos >= 0 ? (uint32_t)nxt_pos : fr_n;
