@@ -37,6 +37,8 @@ struct dd_index {
   uint64_t bcap = 0;        // batch capacity of the scratch below
   uint32_t* new_out = nullptr;
   float* new_key = nullptr;  // distances of new_out's entries (fast form)
+  float* row_key = nullptr;  // n x Rp: each graph entry's distance to its row's point (fast form)
+  bool row_key_ok = false;
   uint32_t* stat_vis = nullptr;
   uint32_t* stat_cmps = nullptr;
   uint32_t* sort_t[2] = {nullptr, nullptr};  // semisort ping-pong buffers
@@ -482,6 +484,7 @@ int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& r
     ra.start = P->start_point;
     ra.new_out = h->new_out;
     ra.new_key = bp.fast ? h->new_key : nullptr;
+    ra.row_key = bp.fast ? h->row_key : nullptr;
     ra.stat_vis = h->stat_vis;
     ra.stat_cmps = h->stat_cmps;
     ra.vis_all = h->vis_all;
@@ -607,7 +610,7 @@ int dd_destroy(dd_index* h) {
   void* ptrs[] = {h->points, h->graph, h->err, h->new_out, h->new_key, h->stat_vis, h->stat_cmps,
                   h->sort_t[0], h->sort_t[1], h->sort_v[0], h->sort_v[1], h->hist, h->heads,
                   h->flags, h->counters, h->big, h->block_sums, h->acc, h->gcand, h->gkey,
-                  h->gpos, h->gbits, h->granges, h->vis_all, h->ref_rows};
+                  h->gpos, h->gbits, h->granges, h->vis_all, h->ref_rows, h->row_key};
   for (void* p : ptrs) dfree(p);
   dfree(h->queues);
   dfree(h->qcls);
@@ -830,6 +833,13 @@ int build_once(dd_index* h, const dd_build_params* P, uint32_t vcap, dd_stats* s
   bp.splan = plan_search(view(h), bp.slay, P->L);
   bp.pplan = plan_prune(view(h), bp.play, bp.fast);
   bp.squeue = bp.pqueue = bp.fast;
+  if (bp.fast && !h->row_key_ok) {
+    // the fast form keeps every graph entry's distance to its row's point
+    // beside the graph, so a reverse prune needs no distance of its row
+    h->scratch_gen++;
+    CK(dalloc(&h->row_key, h->n * (uint64_t)h->Rp));
+    h->row_key_ok = true;
+  }
   rc = ensure_vis_all(h, Bmax * 2ull * vcap);
   if (rc) return rc;
   rc = ensure_queues(h, 2 + 2 * rounds.size() * (P->two_pass ? 2 : 1));
@@ -1009,6 +1019,7 @@ RoundArgs shard_round_args(dd_index* h, uint64_t floor, uint64_t B, uint32_t* ro
   ra.start = h->shard_params.start_point;
   ra.new_out = rows;
   ra.new_key = nullptr;  // the exchanged rows carry no distances: the reverse step recomputes
+  ra.row_key = nullptr;
   ra.stat_vis = h->stat_vis;
   ra.stat_cmps = h->stat_cmps;
   ra.vis_all = h->vis_all;

@@ -18,14 +18,17 @@
 
 namespace ddk {
 
-__global__ void k_apply_rows(uint32_t* graph, const uint32_t* new_out, uint64_t floor,
-                             uint64_t nvec, uint32_t Rp) {
+// row_key (may be null): the rows' distances go beside them (new_key)
+__global__ void k_apply_rows(uint32_t* graph, const uint32_t* new_out, float* row_key,
+                             const float* new_key, uint64_t floor, uint64_t nvec, uint32_t Rp) {
   // rows are Rp uint32 = Rp/4 uint4; batch rows are contiguous in the graph
   const uint4* src = (const uint4*)new_out;
   uint4* dst = (uint4*)(graph + floor * Rp);
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nvec;
-       i += (uint64_t)gridDim.x * blockDim.x)
+       i += (uint64_t)gridDim.x * blockDim.x) {
     dst[i] = src[i];
+    if (row_key) ((float4*)(row_key + floor * Rp))[i] = ((const float4*)new_key)[i];
+  }
 }
 
 // per-warp shared layout of the reverse kernel
@@ -52,6 +55,10 @@ __device__ __forceinline__ void segment_of(const ReverseScratch& rs, uint32_t k,
   end = (k + 1 < rs.counters[1]) ? rs.heads[k + 1] : rs.counters[0];
 }
 
+// the reverse prune's greedy loads the next chunk's rows ahead (with kept
+// row distances no candidate row is read before the greedy)
+constexpr bool kRevPrefetch = true;
+
 // Append the sources of segment [start, end) (already in batch order), or
 // prune when the row would exceed R (one warp; s + deg <= kRevCandCap).
 template <int DT, int MT, bool TC>
@@ -60,15 +67,22 @@ __device__ void reverse_one(const IndexView& ix, const RoundArgs& ra, const Reve
                             PruneSmem Pm) {
   const uint32_t lane = lane_id();
   uint32_t* row = ix.graph + (uint64_t)t * ix.Rp;
+  // the row's distances to t, kept beside the graph (fast form)
+  float* rk = (ra.new_key && ra.row_key) ? ra.row_key + (uint64_t)t * ix.Rp : nullptr;
   const uint32_t* sk = rs.sv + start;
   if (s + deg <= ix.R) {
-    for (uint32_t j = lane; j < s; j += 32) row[deg + j] = (uint32_t)(ra.floor + sk[j] / ix.Rp);
+    for (uint32_t j = lane; j < s; j += 32) {
+      row[deg + j] = (uint32_t)(ra.floor + sk[j] / ix.Rp);
+      if (rk) rk[deg + j] = ra.new_key[sk[j]];
+    }
     __syncwarp();
     return;
   }
-  const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
-  load_vec(tv, ix.points + (uint64_t)t * ix.stride, qb);
-  __syncwarp();
+  if (!rk) {  // otherwise no distance to t is computed here
+    const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
+    load_vec(tv, ix.points + (uint64_t)t * ix.stride, qb);
+    __syncwarp();
+  }
   // a source's distance to t is the one its own prune selected t with (the
   // distances are symmetric bit for bit: (a-b)^2 = (b-a)^2, a*b = b*a, same
   // summation order), when the insert prune kept it
@@ -81,14 +95,13 @@ __device__ void reverse_one(const IndexView& ix, const RoundArgs& ra, const Reve
   for (uint32_t j = lane; j < deg; j += 32) {
     uint32_t c = row[j];
     Pm.cid[s + j] = c;
-    Pm.ckey[s + j] = Dist<DT, MT>::eval(tv, ix.points + (uint64_t)c * ix.stride, ix.d);
+    Pm.ckey[s + j] = rk ? rk[j] : Dist<DT, MT>::eval(tv, ix.points + (uint64_t)c * ix.stride, ix.d);
   }
   __syncwarp();
   const uint32_t m = s + deg;
   warp_std_sort(Pm, m);
-  // the candidate rows were just read for their distances to t: no prefetch
-  warp_greedy_select_fast<DT, MT, false, TC>(ix.points, ix.stride, ix.d, t, Pm, m, ra.alpha, ix.R, row,
-                                         ix.Rp, Pm.sel);
+  warp_greedy_select_fast<DT, MT, kRevPrefetch, TC>(ix.points, ix.stride, ix.d, t, Pm, m, ra.alpha,
+                                                    ix.R, row, ix.Rp, Pm.sel, rk);
   if (lane == 0) {
     atomicAdd(&rs.counters[2], 1u);
     atomicAdd(&rs.counters[3], m);
@@ -167,6 +180,7 @@ __global__ void __launch_bounds__(kBigThreads) k_reverse_big(IndexView ix, Round
     const uint32_t t = rs.st[start];
     const uint32_t s = end - start;
     uint32_t* row = ix.graph + (uint64_t)t * ix.Rp;
+    float* rk = (ra.new_key && ra.row_key) ? ra.row_key + (uint64_t)t * ix.Rp : nullptr;
     if (wid == 0) {
       uint32_t dg = row_degree(row, ix.Rp);
       if (lane == 0) s_deg = dg;
@@ -192,7 +206,7 @@ __global__ void __launch_bounds__(kBigThreads) k_reverse_big(IndexView ix, Round
     for (uint32_t j = tid; j < deg; j += blockDim.x) {
       uint32_t c = row[j];
       cid[s + j] = c;
-      ckey[s + j] = Dist<DT, MT>::eval(tv, ix.points + (uint64_t)c * ix.stride, ix.d);
+      ckey[s + j] = rk ? rk[j] : Dist<DT, MT>::eval(tv, ix.points + (uint64_t)c * ix.stride, ix.d);
     }
     for (uint32_t w = tid; w < (m + 31) / 32; w += blockDim.x) bits[w] = 0;
     if (tid == 0) {
@@ -259,7 +273,7 @@ __global__ void __launch_bounds__(kBigThreads) k_reverse_big(IndexView ix, Round
         Pg.ckey = ckey;
         Pg.sel = (uint4*)gsel;
         warp_greedy_select_mma<DT, MT>(ix.points, ix.stride, ix.d, t, Pg, m, ra.alpha, ix.R, row,
-                                       ix.Rp, Pg.sel);
+                                       ix.Rp, Pg.sel, rk);
         if (lane == 0) {
           atomicAdd(&rs.counters[2], 1u);
           atomicAdd(&rs.counters[3], m);
@@ -273,7 +287,10 @@ __global__ void __launch_bounds__(kBigThreads) k_reverse_big(IndexView ix, Round
       const uint32_t ps = cid[idx];
       idx++;
       if (ps == t || ps == DD_NONE) continue;
-      if (tid == 0) row[nsel] = ps;
+      if (tid == 0) {
+        row[nsel] = ps;
+        if (rk) rk[nsel] = ckey[idx - 1];
+      }
       nsel++;
       const uint8_t* prow = ix.points + (uint64_t)ps * ix.stride;
       for (uint32_t q = idx + tid; q < mm; q += blockDim.x) {
@@ -321,7 +338,8 @@ void launch_apply_rows(const IndexView& ix, const RoundArgs& ra, cudaStream_t st
   uint64_t nvec = (uint64_t)ra.B * ix.Rp / 4;
   if (!nvec) return;
   int grid = (int)std::min<uint64_t>((nvec + 255) / 256, 4096);
-  k_apply_rows<<<grid, 256, 0, st>>>(ix.graph, ra.new_out, ra.floor, nvec, ix.Rp);
+  k_apply_rows<<<grid, 256, 0, st>>>(ix.graph, ra.new_out, ra.new_key ? ra.row_key : nullptr,
+                                     ra.new_key, ra.floor, nvec, ix.Rp);
 }
 
 void launch_reverse(const IndexView& ix, const RoundArgs& ra, const ReverseScratch& rs,

@@ -68,6 +68,8 @@ struct RoundArgs {
   uint32_t* new_out;     // B x Rp
   float* new_key;        // B x Rp distances of new_out's entries to their row's point, or
                          // null (the reverse step then recomputes them)
+  float* row_key;        // with new_key: n x Rp, each graph entry's distance to its row's
+                         // point (kept by every row write of the build), or null
   uint32_t* stat_vis;    // B visited-list lengths (k_search writes, k_prune reads)
   uint32_t* stat_cmps;   // B (may be null)
   uint32_t* vis_all;     // per batch point: vcap visited ids, then vcap distances
