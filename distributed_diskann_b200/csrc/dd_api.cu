@@ -60,6 +60,12 @@ struct dd_index {
   uint32_t* vis_all = nullptr;
   uint64_t vis_all_words = 0;
   uint32_t* ref_rows = nullptr;  // n x (R+1) reference-layout rows for downloads
+  // fast form, float data: BF16 copies of the rows and their squared norms
+  // (the search steps' screen), rebuilt after any change of the points
+  uint8_t* screen = nullptr;
+  float* snorm = nullptr;
+  uint64_t sstride = 0;
+  bool screen_ok = false;
   bool verbose = false;
   bool hash32 = false;  // DD_HASH32=1: 32-bit hash-table ids even when n < 2^24 - 1
   int search_mode = DD_MODE_FAST;
@@ -121,6 +127,25 @@ IndexView view(dd_index* h) {
   return v;
 }
 
+// The BF16 screen of float searches (search_core.cuh screen_and_rerank), for
+// float data of at most 4096 dimensions, is opt-in: DD_SCREEN=1.  Measured on
+// B200 it is slower than computing every candidate's exact FP32 distance (the
+// search is bound by instruction issue, not by the bytes the BF16 rows save:
+// 1M x 200 MIPS build search 286 against 276 ms, queries at recall 0.95 3.1M
+// against 4.2M QPS), so by default the fast form computes them all exactly,
+// as the plain form does.
+bool screen_enabled(const dd_index* h) {
+  if (h->dtype != DD_F32 || h->d > 4096) return false;
+  const char* e = getenv("DD_SCREEN");
+  return e && e[0] == '1';
+}
+
+void attach_screen(const dd_index* h, IndexView* ix) {
+  ix->screen = h->screen;
+  ix->sstride = h->sstride;
+  ix->snorm = h->snorm;
+}
+
 template <typename T>
 cudaError_t dalloc(T** p, uint64_t count) {
   return cudaMalloc((void**)p, std::max<uint64_t>(count, 1) * sizeof(T));
@@ -128,6 +153,20 @@ cudaError_t dalloc(T** p, uint64_t count) {
 
 void dfree(void* p) {
   if (p) cudaFree(p);
+}
+
+// Makes the BF16 row copies current (stream-ordered after the points' upload).
+int ensure_screen(dd_index* h) {
+  if (h->screen_ok) return DD_OK;
+  if (!h->screen) {
+    h->sstride = ((uint64_t)h->d * 2 + 15) / 16 * 16;
+    CK(dalloc(&h->screen, h->n * h->sstride));
+    CK(dalloc(&h->snorm, h->n));
+  }
+  launch_screen_rows(view(h), h->screen, h->sstride, h->snorm, h->stream);
+  CK(cudaGetLastError());
+  h->screen_ok = true;
+  return DD_OK;
 }
 
 int check_error_word(dd_index* h, uint32_t* bits = nullptr) {
@@ -346,6 +385,7 @@ struct BuildPlan {
   PruneLayout play;
   LaunchPlan pplan;
   bool fast;     // DD_MODE_FAST: tensor-core greedy of robustPrune (integer data)
+  bool screen;   // fast form, float data: searches screen candidates on BF16 rows
   bool squeue;   // persistent k_search fed by the round's work queue
   bool pqueue;   // persistent k_prune fed by the round's work queue
 };
@@ -372,7 +412,8 @@ std::vector<std::pair<std::vector<uint64_t>, TuneResult>> g_tune;
 
 std::vector<uint64_t> tune_key(const dd_index* h, const BuildPlan& bp, uint32_t L) {
   return {(uint64_t)h->dtype, (uint64_t)h->metric, h->d, h->Rp, L, bp.slay.vcap, bp.slay.h24,
-          bp.slay.fastf, bp.slay.total, bp.play.total, (uint64_t)bp.fast, (uint64_t)h->device};
+          bp.slay.fastf, bp.slay.total, bp.play.total, (uint64_t)bp.fast, (uint64_t)bp.screen,
+          (uint64_t)h->device};
 }
 
 bool tune_lookup(const std::vector<uint64_t>& key, TuneResult* out) {
@@ -404,6 +445,7 @@ int grid_for(const LaunchPlan& pl, uint64_t B, int sm_count) {
 // for every candidate shape; the work-queue counter used is queues[0].
 int tune_round(dd_index* h, RoundArgs ra, BuildPlan* bp, TuneResult* res) {
   IndexView ix = view(h);
+  if (bp->screen) attach_screen(h, &ix);
   ra.B = std::min<uint32_t>(ra.B, kTuneItems);
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
@@ -472,6 +514,7 @@ int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& r
                 const dd_build_params* P, BuildPlan& bp, uint64_t qbase, PhaseEvents* pe,
                 TuneResult* tune) {
   IndexView ix = view(h);
+  if (bp.screen) attach_screen(h, &ix);
   for (size_t r = 0; r < rounds.size(); r++) {
     const auto& rd = rounds[r];
     uint64_t B = rd.second > rd.first ? rd.second - rd.first : 0;
@@ -610,7 +653,8 @@ int dd_destroy(dd_index* h) {
   void* ptrs[] = {h->points, h->graph, h->err, h->new_out, h->new_key, h->stat_vis, h->stat_cmps,
                   h->sort_t[0], h->sort_t[1], h->sort_v[0], h->sort_v[1], h->hist, h->heads,
                   h->flags, h->counters, h->big, h->block_sums, h->acc, h->gcand, h->gkey,
-                  h->gpos, h->gbits, h->granges, h->vis_all, h->ref_rows, h->row_key};
+                  h->gpos, h->gbits, h->granges, h->vis_all, h->ref_rows, h->row_key,
+                  h->screen, h->snorm};
   for (void* p : ptrs) dfree(p);
   dfree(h->queues);
   dfree(h->qcls);
@@ -646,6 +690,7 @@ int dd_check_errors(dd_index* h) {
 
 int dd_upload_points(dd_index* h, const void* rows, uint64_t row_stride_bytes) {
   if (!h || !rows) return DD_ERR_ARG;
+  h->screen_ok = false;  // the BF16 row copies follow the new points
   uint64_t rb = (uint64_t)h->d * esize(h->dtype);
   if (row_stride_bytes < rb) return fail(h, DD_ERR_ARG, "row stride %llu < row bytes %llu",
                                          (unsigned long long)row_stride_bytes, (unsigned long long)rb);
@@ -658,6 +703,7 @@ int dd_upload_points(dd_index* h, const void* rows, uint64_t row_stride_bytes) {
 
 int dd_upload_points_device(dd_index* h, const void* rows, uint64_t row_stride_bytes) {
   if (!h || !rows) return DD_ERR_ARG;
+  h->screen_ok = false;  // the BF16 row copies follow the new points
   uint64_t rb = (uint64_t)h->d * esize(h->dtype);
   if (row_stride_bytes < rb) return fail(h, DD_ERR_ARG, "row stride too small");
   CK(cudaSetDevice(h->device));
@@ -669,6 +715,7 @@ int dd_upload_points_device(dd_index* h, const void* rows, uint64_t row_stride_b
 
 int dd_upload_points_async(dd_index* h, const void* rows, uint64_t row_stride_bytes) {
   if (!h || !rows) return DD_ERR_ARG;
+  h->screen_ok = false;  // the BF16 row copies follow the new points
   uint64_t rb = (uint64_t)h->d * esize(h->dtype);
   if (row_stride_bytes < rb) return fail(h, DD_ERR_ARG, "row stride %llu < row bytes %llu",
                                          (unsigned long long)row_stride_bytes, (unsigned long long)rb);
@@ -683,6 +730,7 @@ int dd_upload_points_async(dd_index* h, const void* rows, uint64_t row_stride_by
 // the next one is read from disk.
 int dd_load_points_file(dd_index* h, const char* path) {
   if (!h || !path) return DD_ERR_ARG;
+  h->screen_ok = false;  // the BF16 row copies follow the new points
   std::ifstream f(path, std::ios::binary);
   if (!f) return fail(h, DD_ERR_IO, "cannot open %s", path);
   uint32_t hdr[2];
@@ -833,6 +881,11 @@ int build_once(dd_index* h, const dd_build_params* P, uint32_t vcap, dd_stats* s
   bp.splan = plan_search(view(h), bp.slay, P->L);
   bp.pplan = plan_prune(view(h), bp.play, bp.fast);
   bp.squeue = bp.pqueue = bp.fast;
+  bp.screen = bp.fast && screen_enabled(h);
+  if (bp.screen) {
+    rc = ensure_screen(h);
+    if (rc) return rc;
+  }
   if (bp.fast && !h->row_key_ok) {
     // the fast form keeps every graph entry's distance to its row's point
     // beside the graph, so a reverse prune needs no distance of its row
@@ -1007,6 +1060,7 @@ BuildPlan shard_plan(dd_index* h) {
   bp.splan = plan_search(view(h), bp.slay, P->L);
   bp.pplan = plan_prune(view(h), bp.play, bp.fast);
   bp.squeue = bp.pqueue = bp.fast;
+  bp.screen = bp.fast && screen_enabled(h);
   return bp;
 }
 
@@ -1052,6 +1106,10 @@ int dd_shard_begin(dd_index* h, const dd_build_params* P, uint64_t max_batch) {
   if (rc) return rc;
   rc = ensure_queues(h, 2);
   if (rc) return rc;
+  if (bp.screen) {
+    rc = ensure_screen(h);
+    if (rc) return rc;
+  }
   CK(cudaMemsetAsync(h->graph, 0xff, h->n * h->Rp * 4ull, h->stream));
   CK(cudaMemsetAsync(h->err, 0, 4, h->stream));
   CK(cudaStreamSynchronize(h->stream));
@@ -1075,6 +1133,11 @@ int dd_shard_search_prune(dd_index* h, uint64_t lo, uint64_t hi, uint32_t* rows)
     ra.qprune = h->queues + 1;
   }
   IndexView ix = view(h);
+  if (bp.screen) {
+    int rc = ensure_screen(h);
+    if (rc) return rc;
+    attach_screen(h, &ix);
+  }
   launch_search(ix, ra, bp.slay, bp.splan, grid_for(bp.splan, ra.B, h->sm_count), h->stream);
   launch_prune_round(ix, ra, bp.play, bp.slay.vcap, bp.pplan, grid_for(bp.pplan, ra.B, h->sm_count),
                      bp.fast, h->stream);
@@ -1207,6 +1270,12 @@ int dd_search_device(dd_index* h, const void* queries, uint64_t nq, uint64_t qst
   }
   uint32_t* counts = h->qcls + (uint64_t)kQueryClasses * nq;
   uint32_t* queues = counts + kQueryClasses;
+  IndexView ixq = view(h);
+  if (screen_enabled(h)) {  // float data: BF16 screen, exact re-rank
+    int rc = ensure_screen(h);
+    if (rc) return rc;
+    attach_screen(h, &ixq);
+  }
   CK(cudaMemsetAsync(counts, 0, 2 * kQueryClasses * 4, h->stream));
   launch_bin_queries(L_per_query, nq, k, Lmax, h->qcls, counts, h->stream);
   h->launches = 1;
@@ -1241,7 +1310,7 @@ int dd_search_device(dd_index* h, const void* queries, uint64_t nq, uint64_t qst
       }
       qc.hash_scratch = h->qhash;
     }
-    launch_query(view(h), qc, lc, wpc, grid, h->stream);
+    launch_query(ixq, qc, lc, wpc, grid, h->stream);
     h->launches++;
   }
   CK(cudaGetLastError());
@@ -1428,7 +1497,13 @@ int dd_groundtruth(dd_index* h, const void* queries, uint64_t nq, uint64_t qstri
   return DD_OK;
 }
 
-void* dd_device_points(dd_index* h) { return h ? h->points : nullptr; }
+// the caller may write the points through this pointer: the BF16 row copies
+// of the fast float search are rebuilt before their next use
+void* dd_device_points(dd_index* h) {
+  if (!h) return nullptr;
+  h->screen_ok = false;
+  return h->points;
+}
 uint64_t dd_device_row_stride(dd_index* h) { return h ? h->stride : 0; }
 void* dd_device_graph(dd_index* h) { return h ? h->graph : nullptr; }
 uint32_t dd_device_row_len(dd_index* h) { return h ? h->Rp : 0; }

@@ -8,6 +8,8 @@
 #include <climits>
 #include <cstdio>
 
+#include <cuda_bf16.h>
+
 #include "dd_common.cuh"
 #include "kernel_util.cuh"
 #include "kernels.cuh"
@@ -438,6 +440,49 @@ void launch_to_ref_rows(const IndexView& ix, uint32_t* out, cudaStream_t st) {
 void launch_from_ref_rows(const IndexView& ix, const uint32_t* in, cudaStream_t st) {
   int grid = (int)std::min<uint64_t>((ix.n * 32 + 255) / 256, 65536);
   k_from_ref_rows<<<grid, 256, 0, st>>>(ix.graph, ix.n, ix.R, ix.Rp, in, ix.err);
+}
+
+// ============================================================ BF16 row copies
+// One warp per row: each lane converts 8 values (two float4 of the FP32 row)
+// into one 16-byte word of BF16 values; values at or beyond d become zeros.
+// The squared norm of the BF16 row is summed in FP32 (its rounding is far
+// inside the screen's 1% slack on the bound term it enters).
+__global__ void __launch_bounds__(256) k_screen_rows(const uint8_t* points, uint64_t stride,
+                                                     uint64_t n, uint32_t d, uint8_t* screen,
+                                                     uint64_t sstride, float* snorm) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t nw = (d + 7) >> 3;
+  const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t i = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n;
+       i += nwarps) {
+    const float* row = (const float*)(points + i * stride);
+    uint4* out = (uint4*)(screen + i * sstride);
+    float nrm = 0.f;
+    for (uint32_t w = lane; w < nw; w += 32) {
+      uint32_t h[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const uint32_t e = 8 * w + 2 * j;
+        const float x0 = e < d ? __ldg(row + e) : 0.f;
+        const float x1 = e + 1 < d ? __ldg(row + e + 1) : 0.f;
+        const __nv_bfloat16 b0 = __float2bfloat16_rn(x0), b1 = __float2bfloat16_rn(x1);
+        const float f0 = __bfloat162float(b0), f1 = __bfloat162float(b1);
+        nrm = fmaf(f0, f0, nrm);
+        nrm = fmaf(f1, f1, nrm);
+        h[j] = (uint32_t)__bfloat16_as_ushort(b0) | ((uint32_t)__bfloat16_as_ushort(b1) << 16);
+      }
+      out[w] = make_uint4(h[0], h[1], h[2], h[3]);
+    }
+    for (uint32_t w = nw + lane; w < sstride / 16; w += 32) out[w] = make_uint4(0, 0, 0, 0);
+    for (int o = 16; o; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+    if (lane == 0) snorm[i] = nrm;
+  }
+}
+
+void launch_screen_rows(const IndexView& ix, uint8_t* screen, uint64_t sstride, float* snorm,
+                        cudaStream_t st) {
+  const int grid = (int)std::min<uint64_t>((ix.n + 7) / 8, 148 * 16);
+  k_screen_rows<<<grid, 256, 0, st>>>(ix.points, ix.stride, ix.n, ix.d, screen, sstride, snorm);
 }
 
 }  // namespace ddk

@@ -45,6 +45,12 @@ struct IndexView {
   uint64_t n;
   uint32_t d;
   uint32_t* err;
+  // fast form, float data: BF16 copies of the rows (sstride bytes apart) and
+  // the squared norm of each copy, which search steps screen candidates with
+  // (null: every candidate gets its exact distance)
+  const uint8_t* screen = nullptr;
+  uint64_t sstride = 0;
+  const float* snorm = nullptr;
 };
 
 // keep_vis: the query layout reserves the visited list (k_beam keeps it;
@@ -223,5 +229,10 @@ void launch_to_ref_rows(const IndexView& ix, uint32_t* out, cudaStream_t st);
 void launch_from_ref_rows(const IndexView& ix, const uint32_t* in, cudaStream_t st);
 // knn_index::build_index final step: sort each row by distance to its owner
 void launch_sort_rows(const IndexView& ix, cudaStream_t st);
+// fast form, float data: BF16 copies of the rows (round to nearest, zero
+// padded to sstride bytes) and their squared norms, which the search steps'
+// screen reads (search_core.cuh screen_and_rerank)
+void launch_screen_rows(const IndexView& ix, uint8_t* screen, uint64_t sstride, float* snorm,
+                        cudaStream_t st);
 
 }  // namespace ddk

@@ -129,6 +129,9 @@ struct SearchParams {
   int query_mode;       // track evicted visited entries for re-entry
   int keep_visited;     // record the visited list (build / debug)
   uint32_t* err;
+  const uint8_t* screen;  // BF16 rows of float data (IndexView::screen), or null
+  uint64_t sstride;
+  const float* snorm;
 };
 
 struct SearchOut {
@@ -181,6 +184,196 @@ __host__ __device__ inline uint32_t fast_hash_bits(uint32_t L) {
 template <int DT, int MT>
 __device__ __forceinline__ float point_dist(const SearchParams& P, const uint8_t* qv, uint32_t id) {
   return Dist<DT, MT>::eval(qv, P.points + (uint64_t)id * P.stride, P.d);
+}
+
+// ---------------------------------------------------------------------------
+// Fast form, float data: BF16 screen + exact FP32 re-rank of one step's kept
+// neighbours (ids in S.s_id[0, nk)).  A neighbour enters the frontier only if
+// its exact distance (the reference's FP32 order) is below the cutoff
+// (include/utils/beamSearch.h:135-145).  Each neighbour's distance is first
+// estimated from the BF16 copy of its row (half the bytes; G lanes each, any
+// summation order) together with a rigorous bound on how far the exact FP32
+// value can lie from the estimate; a neighbour whose lower bound is already at
+// or above the cutoff fails for certain and is dropped.  The others (the ones
+// that pass, and the few the bound cannot decide) get the exact distance from
+// the FP32 row, one lane each, so every frontier entry carries the reference's
+// value and the search takes the reference's path.
+//
+// The bound (u = 2^-24 is FP32's unit roundoff; b~ = bf16(b) is round to
+// nearest, so |b~_i - b_i| <= 2^-8 |b~_i| for normal values):
+//   L2:   |sum (a_i-b_i)^2 - sum (a_i-b~_i)^2| = |sum e_i (2 t_i + e_i)|
+//         <= 2^-7 sum |b~_i| |t_i| + 2^-16 |b~|^2,     t_i = a_i - b~_i
+//   MIPS: |sum a_i b_i - sum a_i b~_i| <= 2^-8 sum |a_i b~_i|
+// plus the rounding of both FP32 sums: at most (d + 16) 2^-23 (gam) times the
+// sum of the absolute terms, taken three times over for the two sums and the
+// bound's own arithmetic, an extra 2^-20 for the final subtraction and 1e-20
+// for subnormal BF16 values.  A NaN or infinite estimate (data beyond the BF16
+// range) never drops a neighbour: the comparison is written to fail on NaN.
+// Returns the number of candidates written to S.c_id / S.c_d, which hold the
+// same entries in the same (neighbour) order as the exact path would.
+// ---------------------------------------------------------------------------
+// The exact FP32 distance (Dist<DD_F32, MT>::eval's value, bit for bit) from
+// the query q (shared memory) to `row`, computed by a group of G lanes (G =
+// 1, 2, 4 or 8, warp-uniform; sub = lane index in the group).  The reference
+// sums float L2 as a chain over 4-value groups (each group summed left to
+// right) and MIPS as a chain over single products: the terms do not depend on
+// the chain, so the G lanes load and compute them in parallel (the row is in
+// flight at once instead of in G consecutive batches) and every lane of the
+// group then adds them into the chain in the reference's order, taking each
+// term from the lane that computed it by shuffle.  Every lane of the warp
+// must call it; lanes with act == false return 0.
+template <int MT>
+__device__ __forceinline__ float exact_dist_group(const float* q, const float* row, uint32_t d,
+                                                  uint32_t sub, uint32_t G, bool act) {
+  if (G == 1) return act ? Dist<DD_F32, MT>::eval(q, row, d) : 0.f;
+  const uint32_t FULL = 0xffffffffu;
+  const uint32_t base = lane_id() & ~(G - 1u);
+  const uint32_t nv4 = (d + 3) >> 2;  // 4-value words (the query is zero padded to them)
+  const float4* r4 = (const float4*)row;
+  const float4* q4 = (const float4*)q;
+  constexpr int NB = 4;  // words a lane has in flight
+  float r = 0.f;
+  for (uint32_t w0 = 0; w0 < nv4; w0 += NB * G) {
+    float4 y[NB];
+#pragma unroll
+    for (int i = 0; i < NB; i++) {
+      const uint32_t w = w0 + (uint32_t)i * G + sub;
+      y[i] = (act && w < nv4) ? __ldg(r4 + w) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int i = 0; i < NB; i++) {
+      const uint32_t w = w0 + (uint32_t)i * G + sub;
+      const float4 x = w < nv4 ? q4[w] : make_float4(0.f, 0.f, 0.f, 0.f);
+      float e[4];
+      if (MT == DD_L2) {
+        const float t0 = __fsub_rn(x.x, y[i].x), t1 = __fsub_rn(x.y, y[i].y);
+        const float t2 = __fsub_rn(x.z, y[i].z), t3 = __fsub_rn(x.w, y[i].w);
+        e[0] = __fmul_rn(t0, t0); e[1] = __fmul_rn(t1, t1);
+        e[2] = __fmul_rn(t2, t2); e[3] = __fmul_rn(t3, t3);
+      } else {
+        e[0] = __fmul_rn(x.x, y[i].x); e[1] = __fmul_rn(x.y, y[i].y);
+        e[2] = __fmul_rn(x.z, y[i].z); e[3] = __fmul_rn(x.w, y[i].w);
+      }
+      const float s = __fadd_rn(__fadd_rn(__fadd_rn(e[0], e[1]), e[2]), e[3]);
+      // the chain over the words w0 + i G + g, g = 0 .. G-1 (warp-uniform)
+      for (uint32_t g = 0; g < G; g++) {
+        const uint32_t wg = w0 + (uint32_t)i * G + g;
+        if (wg >= nv4) break;
+        if (MT == DD_L2 && 4 * wg + 3 < d) {
+          r = __fadd_rn(r, __shfl_sync(FULL, s, base + g));
+        } else {  // MIPS, and the 0-3 value tail of L2: one value at a time
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            const float v = __shfl_sync(FULL, e[j], base + g);
+            if (4 * wg + (uint32_t)j < d) r = __fadd_rn(r, v);
+          }
+        }
+      }
+    }
+  }
+  if (!act) return 0.f;
+  return MT == DD_L2 ? r : -r;
+}
+
+template <int MT>
+__device__ __forceinline__ uint32_t screen_and_rerank(const SearchParams& P, const SearchSmem& S,
+                                                      uint32_t nk, float cutoff) {
+  const uint32_t lane = lane_id();
+  const uint32_t FULL = 0xffffffffu;
+  const uint32_t nw = (P.d + 7) >> 3;  // 16-byte words of a BF16 row
+  const float* qf = (const float*)S.qv;
+  const float gam3 = 3.f * (float)(P.d + 16) * 0x1p-23f + 0x1p-20f;
+  // G lanes per neighbour: 8 up to 4 neighbours, 4 up to 8, else 2
+  const uint32_t lg = nk <= 4 ? 3u : (nk <= 8 ? 2u : 1u);
+  const uint32_t G = 1u << lg, per = 32u >> lg, sub = lane & (G - 1);
+  constexpr int NB = 4;  // words a lane has in flight
+  uint32_t nm = 0;
+  for (uint32_t k0 = 0; k0 < nk; k0 += per) {
+    const uint32_t k = k0 + (lane >> lg);
+    const bool act = k < nk;
+    const uint32_t id = act ? S.s_id[k] : 0u;
+    const uint4* row = (const uint4*)(P.screen + (uint64_t)id * P.sstride);
+    const float nb2 = (MT == DD_L2 && act && sub == 0) ? __ldg(P.snorm + id) : 0.f;
+    float acc = 0.f, bnd = 0.f;
+    for (uint32_t w0 = sub; w0 < nw; w0 += NB * G) {
+      uint4 y[NB];
+#pragma unroll
+      for (int i = 0; i < NB; i++) {
+        const uint32_t w = w0 + (uint32_t)i * G;
+        y[i] = (act && w < nw) ? __ldg(row + w) : make_uint4(0, 0, 0, 0);
+      }
+#pragma unroll
+      for (int i = 0; i < NB; i++) {
+        const uint32_t w = w0 + (uint32_t)i * G;
+        if (w < nw) {
+          // the query holds whole 4-value groups; values at or beyond d (the
+          // BF16 row's zero padding) are left out, whatever a caller's device
+          // query buffer holds there
+          const float4 qa = *(const float4*)(qf + 8 * w);
+          const float4 qb = (8 * w + 4 < P.d) ? *(const float4*)(qf + 8 * w + 4)
+                                              : make_float4(0.f, 0.f, 0.f, 0.f);
+          float qs[8] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w};
+          if (8 * w + 8 > P.d) {
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+              if (8 * w + (uint32_t)j >= P.d) qs[j] = 0.f;
+          }
+          const uint32_t ys[4] = {y[i].x, y[i].y, y[i].z, y[i].w};
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            const uint32_t hw = ys[j >> 1];
+            const float b = __uint_as_float((j & 1) ? (hw & 0xffff0000u) : (hw << 16));
+            if (MT == DD_L2) {
+              const float t = qs[j] - b;
+              acc = fmaf(t, t, acc);
+              bnd = fmaf(fabsf(b), fabsf(t), bnd);
+            } else {
+              acc = fmaf(qs[j], b, acc);
+              bnd = fmaf(fabsf(qs[j]), fabsf(b), bnd);
+            }
+          }
+        }
+      }
+    }
+    for (uint32_t o = 1; o < G; o <<= 1) {
+      acc += __shfl_xor_sync(FULL, acc, o);
+      bnd += __shfl_xor_sync(FULL, bnd, o);
+    }
+    float lowd;
+    if (MT == DD_L2)
+      lowd = acc - (1.01f * (0x1p-7f * bnd + 0x1p-16f * nb2) + acc * gam3 + 1e-20f);
+    else
+      lowd = -acc - (bnd * (1.01f * 0x1p-8f + gam3) + 1e-20f);
+    const bool maybe = act && sub == 0 && !(lowd >= cutoff);
+    const uint32_t mb = __ballot_sync(FULL, maybe);
+    // in place: every id of this pass was read above, and positions before
+    // nm + popc(mb) are at or below the ones read
+    if (maybe) S.s_id[nm + __popc(mb & lanemask_lt())] = id;
+    nm += __popc(mb);
+  }
+  __syncwarp();
+  // exact distances of the survivors: G lanes each (few survivors) or one lane
+  // each (many); both give the reference's FP32 value (exact_dist_group)
+  const uint32_t lx = nm <= 4 ? 3u : (nm <= 8 ? 2u : (nm <= 16 ? 1u : 0u));
+  const uint32_t perx = 32u >> lx, subx = lane & ((1u << lx) - 1u);
+  uint32_t nc = 0;
+  for (uint32_t k0 = 0; k0 < nm; k0 += perx) {
+    const uint32_t k = k0 + (lane >> lx);
+    const bool act = k < nm;
+    const uint32_t id = act ? S.s_id[k] : 0u;
+    const float dist = exact_dist_group<MT>((const float*)S.qv,
+                                            (const float*)(P.points + (uint64_t)id * P.stride),
+                                            P.d, subx, 1u << lx, act);
+    const bool pass = act && subx == 0 && dist < cutoff;
+    const uint32_t pb = __ballot_sync(FULL, pass);
+    if (pass) {
+      const uint32_t pos = nc + __popc(pb & lanemask_lt());
+      S.c_id[pos] = id;
+      S.c_d[pos] = dist;
+    }
+    nc += __popc(pb);
+  }
+  return nc;
 }
 
 // Runs one beam search on the warp.  `qv` must already hold the query.
@@ -384,7 +577,10 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
     // ---- their distances: G lanes per neighbour for integer data (exact in
     // any grouping), one lane for float data (the reference's summation order)
     uint32_t nc = 0;
-    {
+    if (DT == DD_F32 && P.screen != nullptr && cutoff < int_max_f) {
+      // fast form, float data, full frontier: BF16 screen, exact re-rank
+      nc = screen_and_rerank<MT>(P, S, nk, cutoff);
+    } else {
       const uint32_t lg = (DT == DD_F32) ? 0u : (nk <= 8 ? 2u : (nk <= 16 ? 1u : 0u));
       const uint32_t G = 1u << lg, per = 32u >> lg, sub = lane & (G - 1);
       for (uint32_t k0 = 0; k0 < nk; k0 += per) {

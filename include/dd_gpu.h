@@ -40,7 +40,13 @@ extern "C" {
 /* computation forms (dd_build_params.mode, dd_set_search_mode).  Both give
  * the same graph and the same search results, bit for bit:
  *   DD_MODE_FAST  : tensor-core distance tiles where they apply (INT8 Gram
- *                   tiles of robustPrune for integer data), persistent kernels
+ *                   tiles of robustPrune for integer data), optionally for
+ *                   float data (DD_SCREEN=1 in the environment) a BF16 screen
+ *                   of search candidates with an exact FP32 re-rank of the
+ *                   ones it cannot rule out (a BF16 copy of the points, n x
+ *                   round_up(2d, 16) bytes, is then kept on the device; off
+ *                   by default: slower than exact distances on B200),
+ *                   persistent kernels
  *                   fed by a device work queue, each build captured as one CUDA
  *                   graph, autotuned CTA shapes, queries bucketed by beam width;
  *   DD_MODE_PLAIN : every distance on the CUDA cores, grid-stride kernels

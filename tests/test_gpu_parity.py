@@ -352,3 +352,51 @@ def test_visited_capacity_overflow_reruns_the_build(golden, mode):
     assert st["vcap"] > 128
     assert sha(canon(gi.graph())) == g["cases"]["i8_small"]["graph_sha256"]
     gi.close()
+
+
+def _screen_stress_points(metric, n=6_000, d=40, seed=31):
+    """Float rows that stress the BF16 screen's bound: a mixture at three
+    magnitudes (1e-12, 1, 1e15), rows whose values are exact in BF16 (the
+    estimate is then exact and only the margins decide), near-duplicates a
+    BF16 rounding apart, and exact duplicates (distance 0 at the cutoff)."""
+    rng = np.random.default_rng(seed)
+    base = D.gen_mixture_f32(n, d, 30, seed)
+    third = n // 3
+    base[:third] *= np.float32(1e-12)
+    base[third:2 * third] *= np.float32(1e15)
+    k = n // 10
+    base[2 * third:2 * third + k] = np.round(base[2 * third:2 * third + k] * 4) / 4  # exact in BF16
+    src = rng.integers(2 * third, n, k)
+    nudge = (1 + rng.choice([-1, 1], (k, d)) * np.float32(2 ** -9)).astype(np.float32)
+    base[n - 2 * k:n - k] = base[src] * nudge
+    base[n - k:] = base[rng.integers(0, n - 2 * k, k)]
+    if metric == "mips":
+        base /= np.linalg.norm(base.astype(np.float64), axis=1, keepdims=True).astype(np.float32)
+    return np.ascontiguousarray(base, np.float32)
+
+
+@pytest.mark.parametrize("metric", ["l2", "mips"])
+def test_bf16_screen_keeps_the_exact_graph_and_searches(oracle_mod, monkeypatch, metric):
+    """Fast form, float data, with the opt-in BF16 screen (DD_SCREEN=1): build
+    and query searches screen candidates on BF16 copies of the rows and compute
+    the exact FP32 distance only for those the bound cannot rule out.  Graph,
+    visited counts and query results must be the oracle's, and equal to the
+    fast form without the screen (the default, DD_SCREEN=0)."""
+    base = _screen_stress_points(metric)
+    q = base[::37].copy()
+    og, ost = oracle_mod.build(base, 32, 64, 1.2, metric=metric)
+    oi, ov, oc = oracle_mod.search(base, og, q, 10, 40, metric=metric)
+    runs = []
+    for screen in ("1", "0"):
+        monkeypatch.setenv("DD_SCREEN", screen)
+        gi, graph, st = gpu_build(base, 32, 64, 1.2, metric=metric, mode="fast")
+        np.testing.assert_array_equal(graph, canon(og), err_msg=f"screen={screen}")
+        assert st["visited"] == ost["visited"]
+        gi.set_search_mode("fast")
+        ids, _, vis, cmps = gi.search(q, 10, 40)
+        np.testing.assert_array_equal(ids, oi)
+        np.testing.assert_array_equal(vis, ov)
+        np.testing.assert_array_equal(cmps, oc)
+        runs.append(st)
+        gi.close()
+    assert runs[0]["dist_cmps"] == runs[1]["dist_cmps"]
