@@ -146,6 +146,19 @@ void attach_screen(const dd_index* h, IndexView* ix) {
   ix->snorm = h->snorm;
 }
 
+// Fast form, float data: how many lanes compute one candidate's exact distance
+// in a search step (IndexView::fgroup_lg): one by default; DD_FGROUP=1/2/3
+// (2/4/8 lanes) or 4 (per step) asks for lane groups.  Measured on B200 the
+// groups are slower (1M x 200 MIPS build search 277 ms with one lane, 307 ms
+// per-step groups, 395 ms with pairs): the shuffles of the chain cost more
+// than the L1 wavefronts the shared row loads save.
+uint32_t fast_fgroup(const dd_index* h) {
+  if (h->dtype != DD_F32) return 0;
+  uint32_t lg = 0;
+  if (const char* e = getenv("DD_FGROUP")) lg = (uint32_t)std::min(4, std::max(0, atoi(e)));
+  return lg;
+}
+
 template <typename T>
 cudaError_t dalloc(T** p, uint64_t count) {
   return cudaMalloc((void**)p, std::max<uint64_t>(count, 1) * sizeof(T));
@@ -413,7 +426,7 @@ std::vector<std::pair<std::vector<uint64_t>, TuneResult>> g_tune;
 std::vector<uint64_t> tune_key(const dd_index* h, const BuildPlan& bp, uint32_t L) {
   return {(uint64_t)h->dtype, (uint64_t)h->metric, h->d, h->Rp, L, bp.slay.vcap, bp.slay.h24,
           bp.slay.fastf, bp.slay.total, bp.play.total, (uint64_t)bp.fast, (uint64_t)bp.screen,
-          (uint64_t)h->device};
+          (uint64_t)fast_fgroup(h), (uint64_t)h->device};
 }
 
 bool tune_lookup(const std::vector<uint64_t>& key, TuneResult* out) {
@@ -446,6 +459,7 @@ int grid_for(const LaunchPlan& pl, uint64_t B, int sm_count) {
 int tune_round(dd_index* h, RoundArgs ra, BuildPlan* bp, TuneResult* res) {
   IndexView ix = view(h);
   if (bp->screen) attach_screen(h, &ix);
+  if (bp->fast) ix.fgroup_lg = fast_fgroup(h);
   ra.B = std::min<uint32_t>(ra.B, kTuneItems);
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
@@ -515,6 +529,7 @@ int pass_rounds(dd_index* h, const std::vector<std::pair<uint64_t, uint64_t>>& r
                 TuneResult* tune) {
   IndexView ix = view(h);
   if (bp.screen) attach_screen(h, &ix);
+  if (bp.fast) ix.fgroup_lg = fast_fgroup(h);
   for (size_t r = 0; r < rounds.size(); r++) {
     const auto& rd = rounds[r];
     uint64_t B = rd.second > rd.first ? rd.second - rd.first : 0;
@@ -1138,6 +1153,7 @@ int dd_shard_search_prune(dd_index* h, uint64_t lo, uint64_t hi, uint32_t* rows)
     if (rc) return rc;
     attach_screen(h, &ix);
   }
+  if (bp.fast) ix.fgroup_lg = fast_fgroup(h);
   launch_search(ix, ra, bp.slay, bp.splan, grid_for(bp.splan, ra.B, h->sm_count), h->stream);
   launch_prune_round(ix, ra, bp.play, bp.slay.vcap, bp.pplan, grid_for(bp.pplan, ra.B, h->sm_count),
                      bp.fast, h->stream);
@@ -1276,6 +1292,7 @@ int dd_search_device(dd_index* h, const void* queries, uint64_t nq, uint64_t qst
     if (rc) return rc;
     attach_screen(h, &ixq);
   }
+  ixq.fgroup_lg = fast_fgroup(h);
   CK(cudaMemsetAsync(counts, 0, 2 * kQueryClasses * 4, h->stream));
   launch_bin_queries(L_per_query, nq, k, Lmax, h->qcls, counts, h->stream);
   h->launches = 1;

@@ -128,7 +128,7 @@ __global__ void __launch_bounds__((FASTF && FPL == 4) ? 256 : 512, (FASTF && FPL
   P.d = ix.d; P.start = ra.start; P.L = ra.L; P.k = 0; P.cut = 0.0; P.limit = ix.n;
   P.degree_limit = ix.R; P.hbits = lay.hbits; P.vcap = lay.vcap; P.ecap = 0; P.query_mode = 0;
   P.keep_visited = 1; P.err = ix.err;
-  P.screen = ix.screen; P.sstride = ix.sstride; P.snorm = ix.snorm;
+  P.screen = ix.screen; P.sstride = ix.sstride; P.snorm = ix.snorm; P.fgroup_lg = ix.fgroup_lg;
   const uint32_t qb = r16((uint64_t)ix.d * ElemSize<DT>::v);
   uint64_t cur = gw;
   const uint64_t step = (uint64_t)gridDim.x * wpc;
@@ -176,6 +176,7 @@ __global__ void __launch_bounds__(512) k_query(IndexView ix, QueryArgs qa, WarpL
     P.degree_limit = qa.degree_limit; P.hbits = hash_bits_for(P.L); P.vcap = 0;
     P.ecap = qa.ev_cap; P.query_mode = 1; P.keep_visited = 0; P.err = ix.err;
     P.screen = ix.screen; P.sstride = ix.sstride; P.snorm = ix.snorm;
+    P.fgroup_lg = ix.fgroup_lg;
     load_vec(S.qv, qa.queries + q * qa.qstride, qb);
     __syncwarp();
     SearchOut o = warp_beam_search<DT, MT, FPL, CPL>(P, S, qa.skip_self ? q : (uint64_t)-1);
@@ -221,7 +222,7 @@ __global__ void __launch_bounds__(32) k_beam(IndexView ix, BeamArgs ba, WarpLayo
     P.d = ix.d; P.start = ba.start; P.L = ba.L; P.k = ba.k; P.cut = ba.cut; P.limit = ba.limit;
     P.degree_limit = ba.degree_limit; P.hbits = lay.hbits; P.vcap = lay.vcap; P.ecap = lay.vcap;
     P.query_mode = ba.k > 0; P.keep_visited = 1; P.err = ix.err;
-    P.screen = nullptr; P.sstride = 0; P.snorm = nullptr;  // the plain form
+    P.screen = nullptr; P.sstride = 0; P.snorm = nullptr; P.fgroup_lg = 0;  // the plain form
     load_vec(S.qv, ba.queries + q * ba.qstride, qb);
     __syncwarp();
     SearchOut o = warp_beam_search<DT, MT, 16, 4>(P, S, (uint64_t)ba.self_ids[q]);

@@ -51,6 +51,10 @@ struct IndexView {
   const uint8_t* screen = nullptr;
   uint64_t sstride = 0;
   const float* snorm = nullptr;
+  // fast form, float data: log2 of the lanes that compute one candidate's
+  // exact distance in a search step (0: one lane, the plain form; 4: chosen
+  // per step from the candidate count)
+  uint32_t fgroup_lg = 0;
 };
 
 // keep_vis: the query layout reserves the visited list (k_beam keeps it;

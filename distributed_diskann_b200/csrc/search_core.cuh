@@ -132,6 +132,7 @@ struct SearchParams {
   const uint8_t* screen;  // BF16 rows of float data (IndexView::screen), or null
   uint64_t sstride;
   const float* snorm;
+  uint32_t fgroup_lg;     // float data: lanes per row of the exact distances (IndexView)
 };
 
 struct SearchOut {
@@ -581,14 +582,29 @@ __device__ SearchOut warp_beam_search(const SearchParams& P, const SearchSmem& S
       // fast form, float data, full frontier: BF16 screen, exact re-rank
       nc = screen_and_rerank<MT>(P, S, nk, cutoff);
     } else {
-      const uint32_t lg = (DT == DD_F32) ? 0u : (nk <= 8 ? 2u : (nk <= 16 ? 1u : 0u));
+      // float data: one lane per row in the plain form; in the fast form
+      // (fgroup_lg > 0) groups of lanes that load a row together and chain its
+      // terms in the reference's order (exact_dist_group): fewer L1 wavefronts
+      // per row for more shuffles.  fgroup_lg 1-3: G = 2, 4, 8 lanes; 4: the
+      // integer rule (as many lanes as keep one pass, up to 8)
+      const uint32_t fg = P.fgroup_lg;
+      const uint32_t lg =
+          (DT == DD_F32)
+              ? (fg < 4 ? fg : (nk <= 4 ? 3u : (nk <= 8 ? 2u : (nk <= 16 ? 1u : 0u))))
+              : (nk <= 8 ? 2u : (nk <= 16 ? 1u : 0u));
       const uint32_t G = 1u << lg, per = 32u >> lg, sub = lane & (G - 1);
       for (uint32_t k0 = 0; k0 < nk; k0 += per) {
         const uint32_t k = k0 + (lane >> lg);
         const bool act = k < nk;
         const uint32_t id = act ? S.s_id[k] : 0u;
-        const float dist = dist_group<DT, MT, FASTF ? 4 : 8>(
-            (const uint4*)S.qv, P.points + (uint64_t)id * P.stride, P.d, sub, G, act);
+        float dist;
+        if (DT == DD_F32 && fg != 0)
+          dist = exact_dist_group<MT>((const float*)S.qv,
+                                      (const float*)(P.points + (uint64_t)id * P.stride), P.d,
+                                      sub, G, act);
+        else
+          dist = dist_group<DT, MT, FASTF ? 4 : 8>(
+              (const uint4*)S.qv, P.points + (uint64_t)id * P.stride, P.d, sub, G, act);
         const bool pass = act && sub == 0 && dist < cutoff;
         const uint32_t pb = __ballot_sync(FULL, pass);
         if (pass) {

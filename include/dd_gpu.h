@@ -45,7 +45,8 @@ extern "C" {
  *                   of search candidates with an exact FP32 re-rank of the
  *                   ones it cannot rule out (a BF16 copy of the points, n x
  *                   round_up(2d, 16) bytes, is then kept on the device; off
- *                   by default: slower than exact distances on B200),
+ *                   by default: slower than exact distances on B200; so is
+ *                   DD_FGROUP, exact float distances by lane groups),
  *                   persistent kernels
  *                   fed by a device work queue, each build captured as one CUDA
  *                   graph, autotuned CTA shapes, queries bucketed by beam width;
