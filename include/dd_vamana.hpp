@@ -51,12 +51,14 @@ inline ErrorHandler& error_handler_slot() {
 // A handler replaces the print-and-abort default (it may throw).
 inline void set_error_handler(ErrorHandler h) { error_handler_slot() = h; }
 
-inline void check(dd_index* h, int rc, const char* what) {
-  if (rc == DD_OK) return;
+// true when rc is DD_OK; otherwise the handler runs (if it returns, the
+// calling entry point stops where it is and returns) or the process aborts
+inline bool check(dd_index* h, int rc, const char* what) {
+  if (rc == DD_OK) return true;
   const char* msg = h ? dd_last_error(h) : "no handle (the call could not create one)";
   if (ErrorHandler eh = error_handler_slot()) {
     eh(what, rc, msg);
-    return;
+    return false;
   }
   std::printf("ERROR in %s (status %d): %s\n", what, rc, msg);
   std::abort();
@@ -86,6 +88,7 @@ class Index {
   Index(int dtype, int metric, uint64_t n, uint32_t d, uint32_t R, int device = 0) {
     check(nullptr, dd_create(dtype, metric, n, d, R, device, &h_), "dd_create");
   }
+  Index() = default;
   Index(Index&& o) noexcept : h_(o.h_) { o.h_ = nullptr; }
   Index& operator=(Index&& o) noexcept {
     std::swap(h_, o.h_);
@@ -109,11 +112,11 @@ Index upload(PR& Points, uint32_t R, int device = 0) {
   using T = value_t<PR>;
   Index ix(dtype_of<T>(), metric_of<Point>(), (uint64_t)Points.size(), (uint32_t)Points.get_dims(),
            R, device);
-  if (ix)
-    check(ix.get(),
-          dd_upload_points(ix.get(), Points.values.get(),
-                           (uint64_t)Points.aligned_dimension() * sizeof(T)),
-          "dd_upload_points");
+  if (ix && !check(ix.get(),
+                   dd_upload_points(ix.get(), Points.values.get(),
+                                    (uint64_t)Points.aligned_dimension() * sizeof(T)),
+                   "dd_upload_points"))
+    return Index();
   return ix;
 }
 
@@ -137,8 +140,8 @@ void bsp_build(BP& BP_, Graph& G, PR& Points, DP& dp, int device = 0, dd_stats* 
   p.start_point = (uint32_t)dp.start_point_index;
   p.collect_stats = stats != nullptr;
   p.mode = mode;
-  check(ix.get(), dd_build(ix.get(), &p, stats), "dd_build");
-  check(ix.get(), dd_download_graph(ix.get(), graph_rows(G)), "dd_download_graph");
+  if (!check(ix.get(), dd_build(ix.get(), &p, stats), "dd_build")) return;
+  if (!check(ix.get(), dd_download_graph(ix.get(), graph_rows(G)), "dd_download_graph")) return;
   if (dp.save) check(ix.get(), dd_save_graph_file(ix.get(), dp.output_path.c_str()), "Graph::save");
 }
 
@@ -157,7 +160,7 @@ void knn_build_index(BP& BP_, Graph& G, PR& Points, int device = 0, dd_stats* st
   p.two_pass = BP_.two_pass ? 1 : 0;
   p.collect_stats = stats != nullptr;
   p.mode = mode;
-  check(ix.get(), dd_build(ix.get(), &p, stats), "dd_build");
+  if (!check(ix.get(), dd_build(ix.get(), &p, stats), "dd_build")) return;
   check(ix.get(), dd_download_graph(ix.get(), graph_rows(G)), "dd_download_graph");
 }
 
@@ -175,8 +178,9 @@ std::vector<uint32_t> search_all(PR& Query_Points, Graph& G, PR& Base_Points, ui
   std::vector<uint32_t> ids((size_t)nq * (size_t)qp.k);
   Index ix = upload<Point>(Base_Points, (uint32_t)G.max_degree(), device);
   if (!ix) return ids;
-  check(ix.get(), dd_upload_graph(ix.get(), graph_rows(G)), "dd_upload_graph");
-  check(ix.get(), dd_set_search_mode(ix.get(), mode), "dd_set_search_mode");
+  if (!check(ix.get(), dd_upload_graph(ix.get(), graph_rows(G)), "dd_upload_graph") ||
+      !check(ix.get(), dd_set_search_mode(ix.get(), mode), "dd_set_search_mode"))
+    return ids;
   std::vector<uint32_t> Ls((size_t)nq, (uint32_t)qp.beamSize);
   std::vector<float> dists(ids.size());
   if (visited) visited->assign((size_t)nq, 0);
