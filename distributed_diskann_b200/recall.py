@@ -173,7 +173,10 @@ def search_and_parse(search, n: int, max_degree: int, gt_ids, gt_dists, k: int =
 
 
 def gpu_searcher(gi, queries, start: int = 0):
-    """searchAll on a GpuIndex (dd_search) in the sweep's calling form."""
+    """searchAll on a GpuIndex (dd_search) in the sweep's calling form.  Each
+    call copies the queries to the device and the results back, as the
+    reference's timed searchAll takes host queries; bench.py times the device
+    search alone (dd_search_device) for its QPS figures."""
     def search(QP: QueryParams):
         ids, _, vis, cmps = gi.search(queries, QP.k, QP.beamSize, cut=QP.cut, limit=QP.limit,
                                       degree_limit=QP.degree_limit, start=start)
