@@ -95,3 +95,36 @@ def test_oracle_schedule(oracle_mod):
     assert all(c - f <= 1_000_000 for f, c in s)
     s = O.schedule(5_000, max_build=4_000, xita=0.02)
     assert s[-1][1] == 4_000 and max(c - f for f, c in s) == 80
+
+
+def test_oracle_matches_full_size_reference_build_with_limits(oracle_mod):
+    """The oracle at the full size of the 100,000 x 64 f32 mixture workload
+    (R=48, L=96, alpha=1.2) against the reference's own build of the same
+    points (tests/golden/golden_full.json, made by make_golden_full.py from the
+    unmodified sources): the graph digest, and searchAll's ids and visited /
+    dist_cmps sums at several beam widths with and without `limit` (stop after
+    that many visits, include/utils/beamSearch.h:108) and `degree_limit`
+    (scan only the first neighbours of a row, :123)."""
+    import json
+    import os
+
+    from tests.golden.make_golden_full import case_data
+
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden_full.json")
+    rec = json.load(open(here))["cases"]["mix64-f32"]
+    w = D.WORKLOADS["mix64-f32"]
+    base, queries = case_data("mix64-f32")
+    assert sha(base) == rec["input_sha256"], "input generator changed"
+    graph, _ = oracle_mod.build(base, w.R, w.L, w.alpha, metric=w.metric)
+    graph = canon(graph)
+    assert sha(graph) == rec["graph_sha256"]
+    q = queries[: rec["nsearch"]]
+    assert any(s["limit"] for s in rec["search"]) and any(s["degree_limit"] for s in rec["search"])
+    for s in rec["search"]:
+        ids, vis, cmps = oracle_mod.search(base, graph, q, s["k"], s["L"], cut=1.35,
+                                           metric=w.metric, limit=s["limit"],
+                                           degree_limit=s["degree_limit"])
+        tag = f"L={s['L']} limit={s['limit']} degree_limit={s['degree_limit']}"
+        assert sha(ids) == s["ids_sha256"], tag
+        assert int(vis.sum()) == s["visited_sum"], tag
+        assert int(cmps.sum()) == s["cmps_sum"], tag
